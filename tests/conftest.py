@@ -1,0 +1,71 @@
+"""Shared fixtures: the oracle library (built from oracle/ta3_oracle.c if
+absent), the golden vectors, and the `gpu` marker."""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+ORACLE_SO = os.path.join(ROOT, "oracle", "_build", "libta3oracle.so")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+def ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def f32_from_hex(h: str) -> np.float32:
+    return np.frombuffer(bytes.fromhex(h)[::-1], dtype=np.float32)[0]
+
+
+def weights_from_hex(rows) -> np.ndarray:
+    return np.array([[f32_from_hex(h) for h in row] for row in rows], dtype=np.float32)
+
+
+def load_golden(name: str):
+    with open(os.path.join(GOLDEN, f"{name}.json")) as f:
+        return json.load(f)
+
+
+def _load_oracle():
+    if not os.path.exists(ORACLE_SO):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
+    lib = C.CDLL(ORACLE_SO)
+    lib.ta3o_evaluate.restype = C.c_float
+    return lib
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    return _load_oracle()
+
+
+@pytest.fixture(scope="session")
+def golden_games():
+    return load_golden("games")
+
+
+def oracle_eval(lib, w: np.ndarray, seeds: np.ndarray, max_moves: int, threads: int = 8):
+    """Batch through the oracle: model-major (score, pieces, lines, total evals)."""
+    w = np.ascontiguousarray(w, dtype=np.float32).reshape(-1, 97)
+    seeds = np.ascontiguousarray(seeds, dtype=np.uint64)
+    n = w.shape[0] * seeds.size
+    sc = np.zeros(n, np.float32)
+    pc = np.zeros(n, np.uint32)
+    lc = np.zeros(n, np.uint32)
+    ev = C.c_uint64()
+    lib.ta3o_eval_mt(ptr(w), w.shape[0], ptr(seeds), seeds.size, max_moves, threads, ptr(sc), ptr(pc), ptr(lc),
+                     C.byref(ev))
+    return sc, pc, lc, ev.value
