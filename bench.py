@@ -1,0 +1,336 @@
+"""Benchmark: beam placements/s of one CMA-ES generation's evaluation on B200.
+
+One step = one generation of configs[1]: 4 islands x 50 candidates x 50 games =
+10,000 (model, game) sims, v11 weights, cap 2,000 pieces, every game played
+with the depth-4 beam (16/32/32) to the cap or top-out. The unit is the
+evaluated beam placement (one value-model call inside search_move_beam), an
+algorithmic count that is identical on GPU and CPU because the decisions are
+bit-identical.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours       value: kernel-only, inputs resident in HBM, CUDA events on the launch
+           stream, L2 flushed between timed steps; e2e: the public API
+           (ta3b_eval_islands) from pinned host buffers, copies included.
+reference  the reference's own CPU path (oracle/_ref, compiled from the
+           reference sources) on all host threads, bounded sample per step.
+For N > 1 (torchrun) every rank evaluates its own generation (weak scaling,
+no data-path collective); value = all ranks' placements / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from tetris_ai3_b200 import workload  # noqa: E402
+
+METRIC = "beam placements/s on 1 B200 (configs[1]: one CMA-ES generation, 10k sims, cap 2000)"
+UNIT = "placements/s"
+# Lane-instructions the kernel executes per evaluated placement (ncu
+# smsp__thread_inst_executed.sum / placements of the same launch), used for the
+# issue roofline; see profiles/ for the capture it comes from.
+LANE_INSTR_PER_PLACEMENT = float(os.environ.get("TA3B_LANE_INSTR_PER_PLACEMENT", "0") or 0)
+
+
+def _dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
+        int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no nvidia-smi"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace('.', '').isdigit())
+                if any(r[3].replace('.', '').isdigit() for r in rows) else None}
+
+
+def _ref_lib():
+    """The reference's CPU path (oracle/_ref) if built, else the oracle's restatement."""
+    ref = os.path.join(ROOT, "oracle", "_ref", "libta3ref.so")
+    if os.path.exists(ref):
+        return C.CDLL(ref), "ta3ref_eval_mt", "reference"
+    port = os.path.join(ROOT, "oracle", "_build", "libta3oracle.so")
+    if not os.path.exists(port):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
+    return C.CDLL(port), "ta3o_eval_mt", "port"
+
+
+def cpu_rate(batch: workload.Batch, budget_s: float, threads: int):
+    """Placements/s of the CPU path over a bounded sample of the batch: whole
+    models of island 0 (each with its island's games), in workload order,
+    `threads` host threads over the (model, game) pairs, until budget_s."""
+    lib, fn, kind = _ref_lib()
+    f = getattr(lib, fn)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    games = batch.games
+    mpi = batch.models // batch.islands
+    per_chunk = max(1, threads // games)
+    total_ev, models, t_used = 0, 0, 0.0
+    while t_used < budget_s and models < mpi:
+        c = min(per_chunk, mpi - models)
+        w = np.ascontiguousarray(batch.weights[models:models + c], np.float32)
+        seeds = np.ascontiguousarray(batch.seeds[0], np.uint64)
+        sc = np.zeros(c * games, np.float32)
+        evs = C.c_uint64()
+        t0 = time.perf_counter()
+        f(p(w), c, p(seeds), games, batch.max_moves, threads, p(sc), None, None, C.byref(evs))
+        t_used += time.perf_counter() - t0
+        total_ev += evs.value
+        models += c
+    return total_ev / t_used, kind, models * games, t_used
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference(args):
+    rank, world, _ = _dist_env()
+    if rank != 0:
+        return
+    batch = workload.config1()
+    threads = host_threads()
+    rates = []
+    kind = "reference"
+    sample_desc = ""
+    for step in range(args.warmup + args.steps):
+        r, kind, sims, t = cpu_rate(batch, budget_s=args.ref_budget, threads=threads)
+        if step >= args.warmup:
+            rates.append(r)
+            sample_desc = f"first {sims} sims of configs[1] (island 0, model-major), cap 2000, {t:.1f} s per step"
+    v = float(np.mean(rates))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "fp32+int32", "data": "synthetic",
+            "config": {"workload": batch.name, "global_batch": batch.sims, "seq_len": batch.max_moves,
+                       "parallelism": f"{threads} host threads", "cpu": _cpu_model()},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample_desc},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def _cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from tetris_ai3_b200 import ModelEvaluator
+
+    rank, world, local = _dist_env()
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+    # weak scaling: each rank scores its own generation (islands seeded per rank)
+    batch = workload.config1(seed=1 + rank)
+    ev = ModelEvaluator(device=local)
+    stream = torch.cuda.Stream(device=dev)
+    w_dev = torch.from_numpy(batch.weights).to(dev)
+    s_dev = torch.from_numpy(batch.seeds.view(np.int64)).to(dev)
+    n = batch.sims
+    score = torch.empty(n, dtype=torch.float32, device=dev)
+    pieces = torch.empty(n, dtype=torch.int32, device=dev)
+    lines = torch.empty(n, dtype=torch.int32, device=dev)
+    evals = torch.empty(n, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)   # > 126 MB L2
+    torch.cuda.synchronize()
+
+    def step():
+        ev.eval_device(w_dev, s_dev, batch.max_moves, score, pieces, lines, evals, num_islands=batch.islands,
+                       stream=stream)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms = []
+    placements = 0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            with torch.cuda.stream(stream):
+                step()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+            placements += int(evals.to(torch.int64).sum().item())
+    torch.cuda.synchronize()
+    clocks = clk.summary()
+    t_local = sum(ms) / 1000.0
+    t_max = t_local
+    total_pl = placements
+    if world > 1:
+        tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        pt = torch.tensor([placements], device=dev, dtype=torch.float64)
+        dist.all_reduce(pt, op=dist.ReduceOp.SUM)
+        total_pl = int(pt.item())
+    value = total_pl / t_max
+
+    # ---- end to end through the public API: pinned host buffers in, host results out
+    h_w = torch.from_numpy(batch.weights).pin_memory()
+    h_s = torch.from_numpy(batch.seeds.view(np.int64)).pin_memory()
+    h_sc = torch.empty(n, dtype=torch.float32).pin_memory()
+    h_pc = torch.empty(n, dtype=torch.int32).pin_memory()
+    h_lc = torch.empty(n, dtype=torch.int32).pin_memory()
+    lib = ev._lib
+    vp = lambda t: C.c_void_p(t.data_ptr())
+    e2e_steps = max(1, min(args.steps, 3))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        rc = lib.ta3b_eval_islands(ev._ctx, vp(h_w), batch.islands, batch.models // batch.islands, 97, vp(h_s),
+                                   batch.games, batch.max_moves, vp(h_sc), vp(h_pc), vp(h_lc))
+        if rc:
+            raise RuntimeError(lib.ta3b_last_error(ev._ctx).decode())
+    e2e_t = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    assert h_sc.numpy().tobytes() == score.cpu().numpy().tobytes(), "e2e results differ from the device run"
+    e2e_value = (total_pl / args.steps) * e2e_steps / e2e_t
+    h2d = batch.weights.nbytes + batch.seeds.nbytes
+    d2h = n * (4 + 4 + 4)
+
+    if rank == 0:
+        peaks, kind = _peaks()
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
+        peak_issue = sms * 4 * 32 * sm_mhz * 1e6 / 1e12            # lane-instructions, T/s
+        per_gpu = value / world
+        roof = None
+        if LANE_INSTR_PER_PLACEMENT > 0:
+            ach = per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12
+            roof = {"bound": "issue", "achieved": ach, "peak": peak_issue, "unit": "T lane-instr/s",
+                    "frac": ach / peak_issue, "traffic": None,
+                    "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz from MEASURED_PEAKS.json "
+                                   f"({kind})",
+                    "lane_instr_per_placement": LANE_INSTR_PER_PLACEMENT}
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            threads = host_threads()
+            r, ck, sims, t = cpu_rate(batch, budget_s=args.cpu_budget, threads=threads)
+            cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": ck,
+                   "sample": f"first {sims} sims of configs[1] (island 0, model-major), cap 2000, {t:.1f} s"}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32+int32", "data": "synthetic",
+                "config": {"workload": batch.name, "global_batch": batch.sims * world, "seq_len": batch.max_moves,
+                           "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                           "l2": "flushed (256 MB write) between timed steps",
+                           "launch": ev.launch_info()},
+                "sims_per_step": batch.sims, "placements_per_step": total_pl / args.steps / world,
+                "clocks": clocks, "roofline": roof, "cpu_baseline": cpu,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": e2e_steps},
+                "gpu_launches": args.steps}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--ref-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,110 @@
+/*
+ * ta3b.h -- C ABI of the B200 model x game beam-search evaluator.
+ *
+ * Drop-in for the reference's evaluator seam: a population of value-model
+ * weight vectors plus game seeds go in; per-(model, game) score, piece count
+ * and line count come out. Every game is played with the reference's depth-4
+ * beam search (widths 16/32/32) on the 10x23 bit-board with hold and a 5-piece
+ * preview, bit-exact with the reference CPU path.
+ *
+ * Plain C types only (no CUDA or torch types), so cgo / JNI / ctypes / a C++
+ * host can bind it directly. All functions return TA3B_OK (0) or a negative
+ * TA3B_ERR_* code; the message is available from ta3b_last_error(ctx).
+ *
+ * Threading: a context is NOT thread-safe (same contract as the reference's
+ * ta3::gpu::ModelEvaluator, ta3_gpu/incl/ta3/gpu/model_eval.hpp:21-26); use one
+ * context per host thread. Separate contexts may run concurrently; each owns
+ * its own CUDA stream and device buffers.
+ */
+#ifndef TA3B_H
+#define TA3B_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TA3B_NUM_PARAMS 97 /* v11 value model, ta3_ai/incl/ta3/ai/models/models/model_v11.hpp:44 */
+
+enum {
+    TA3B_OK = 0,
+    TA3B_ERR_ARG = -1,     /* bad size, null pointer, parameter-count mismatch */
+    TA3B_ERR_CUDA = -2,    /* a CUDA runtime call failed (message has the CUDA error string) */
+    TA3B_ERR_NODEV = -3,   /* no usable sm_100 device */
+    TA3B_ERR_DEVICE = -4,  /* the kernel reported an error status */
+};
+
+typedef struct ta3b_ctx ta3b_ctx;
+
+typedef struct {
+    int device;                /* CUDA device ordinal */
+    uint32_t warps_per_block;  /* 0 = tuned default */
+    uint32_t blocks_per_sm;    /* 0 = as many as fit */
+} ta3b_config;
+
+/* Create an evaluation context (stream + grow-only device buffers).
+ * Replaces ModelEvaluator::ModelEvaluator(), ta3_gpu/src/cuda/model_eval.cu:92.
+ * Returns NULL on failure; ta3b_last_error(NULL) then holds the reason. */
+ta3b_ctx* ta3b_create(const ta3b_config* cfg);
+
+/* Release the context. Replaces ModelEvaluator::~ModelEvaluator, model_eval.cu:72-83,93. */
+void ta3b_destroy(ta3b_ctx* ctx);
+
+/* Message of the last failure on this context (or of ta3b_create when ctx is NULL). */
+const char* ta3b_last_error(const ta3b_ctx* ctx);
+
+/* Batched evaluation with host buffers: num_models models, each played on the
+ * SAME num_games seeds. weights is model-major, num_models * num_params floats
+ * (num_params must be TA3B_NUM_PARAMS). Outputs are model-major: index
+ * m * num_games + g holds model m on game g. pieces_out, lines_out may be NULL.
+ * score is the reference's score_v1 (FP64, rounded to float); -1e6 when no
+ * piece was placed.
+ * Replaces std::vector<float> ModelEvaluator::eval(std::span<const float> weights,
+ * uint32_t num_models, std::span<const uint64_t> seeds, uint32_t max_moves),
+ * ta3_gpu/incl/ta3/gpu/model_eval.hpp:46-51 / ta3_gpu/src/cuda/model_eval.cu:97-153. */
+int ta3b_eval(ta3b_ctx* ctx, const float* weights, uint32_t num_models, uint32_t num_params,
+              const uint64_t* seeds, uint32_t num_games, uint32_t max_moves,
+              float* score_out, uint32_t* pieces_out, uint32_t* lines_out);
+
+/* Island-batched evaluation in ONE launch: island i owns models
+ * [i*models_per_island, (i+1)*models_per_island) and plays seeds
+ * [i*num_games, (i+1)*num_games). Identical results to one ta3b_eval per
+ * island. This is how one CMA-ES generation of several islands is scored
+ * (ta3_trainer/src/tetris_problem2.cpp:29-72 calls eval once per island batch). */
+int ta3b_eval_islands(ta3b_ctx* ctx, const float* weights, uint32_t num_islands, uint32_t models_per_island,
+                      uint32_t num_params, const uint64_t* seeds, uint32_t num_games, uint32_t max_moves,
+                      float* score_out, uint32_t* pieces_out, uint32_t* lines_out);
+
+/* Device-resident variant of ta3b_eval_islands: every pointer is device memory;
+ * enqueued on `stream` (a cudaStream_t, NULL = the context's stream) and NOT
+ * synchronised. evals_out (may be NULL) receives per-sim counts of evaluated
+ * beam placements (value-model calls). Used for HBM-resident batches and CUDA
+ * graph capture. No reference counterpart (the reference stages host buffers). */
+int ta3b_eval_device(ta3b_ctx* ctx, const float* d_weights, uint32_t num_islands, uint32_t models_per_island,
+                     uint32_t num_params, const uint64_t* d_seeds, uint32_t num_games, uint32_t max_moves,
+                     float* d_score, uint32_t* d_pieces, uint32_t* d_lines, uint32_t* d_evals, void* stream);
+
+/* Per-move trace of every sim (debug / parity tooling): trace_out receives
+ * 3 bytes per move (hold, orientation, x + 2), max_moves moves per sim,
+ * model-major; n_moves_out the number of searched moves per sim;
+ * board_out the final 10 bit-columns per sim. Host buffers. */
+int ta3b_eval_trace(ta3b_ctx* ctx, const float* weights, uint32_t num_models, uint32_t num_params,
+                    const uint64_t* seeds, uint32_t num_games, uint32_t max_moves,
+                    float* score_out, uint32_t* pieces_out, uint32_t* lines_out, uint32_t* evals_out,
+                    uint8_t* trace_out, uint32_t* n_moves_out, uint32_t* board_out);
+
+/* The seeds ta3::gpu::simulate derives for `games` games from one seed
+ * (xoshiro256** draws), ta3_gpu/incl/ta3/gpu/model_eval.hpp:84-103. Host only. */
+int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out);
+
+/* Launch shape the context uses (after the first evaluation): grid blocks,
+ * warps per block, sims per launch. For tooling and the autotuner. */
+int ta3b_launch_info(const ta3b_ctx* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TA3B_H */

@@ -1,0 +1,133 @@
+"""Parity of the CUDA evaluator (through the C ABI) with the reference:
+golden vectors from the reference's own CPU code, the oracle on seeded random
+inputs, and size-independent properties at full configuration sizes.
+Bit-exact throughout: scores compare as float32 bit patterns."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import f32_from_hex, oracle_eval, weights_from_hex
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ev():
+    from tetris_ai3_b200 import ModelEvaluator
+    e = ModelEvaluator(device=0)
+    yield e
+    e.close()
+
+
+def _check_golden_case(ev, case):
+    w = weights_from_hex(case["weights"])
+    seeds = np.array([int(s) for s in case["seeds"]], np.uint64)
+    out = ev.eval_trace(w, w.shape[0], seeds, case["max_moves"])
+    flat = [r for row in case["results"] for r in row]
+    for i, r in enumerate(flat):
+        where = f'{case["name"]} sim {i}'
+        nm = int(out["moves"][i])
+        assert bytes(out["trace"][i][:3 * nm]).hex() == r["trace"], where
+        assert out["score"][i].tobytes() == f32_from_hex(r["score"]).tobytes(), where
+        assert (int(out["pieces"][i]), int(out["lines"][i]), int(out["evals"][i]), nm) == \
+               (r["pieces"], r["lines"], r["evals"], r["moves"]), where
+        assert out["board"][i].tolist() == r["board"], where
+
+
+def test_golden_games_bit_exact(ev, golden_games):
+    for case in golden_games["cases"]:
+        _check_golden_case(ev, case)
+
+
+def test_config0_matches_golden(ev, golden_games):
+    from tetris_ai3_b200 import workload
+    b = workload.config0()
+    case = golden_games["cases"][0]
+    assert np.array_equal(weights_from_hex(case["weights"]), b.weights)
+    sc, pc, lc = ev.eval_full(b.weights, 1, b.seeds[0], b.max_moves)
+    flat = case["results"][0]
+    assert [x.tobytes() for x in sc] == [f32_from_hex(r["score"]).tobytes() for r in flat]
+    assert pc.tolist() == [r["pieces"] for r in flat]
+    assert lc.tolist() == [r["lines"] for r in flat]
+
+
+def test_batched_equals_per_model(ev):
+    # ta3_gpu/tests/src/parity_test.cpp:70-100
+    from tetris_ai3_b200 import workload
+    w = np.stack([(0.7 * workload.normal(300 + m, 97)).astype(np.float32) for m in range(5)])
+    seeds = np.array([1, 2, 3, 4], np.uint64)
+    batched = ev.eval_full(w, 5, seeds, 200)
+    for m in range(5):
+        single = ev.eval_full(w[m], 1, seeds, 200)
+        for a, b in zip(batched, single):
+            assert a[m * 4:(m + 1) * 4].tobytes() == b.tobytes()
+
+
+def test_random_models_match_oracle(ev, oracle):
+    from tetris_ai3_b200 import workload
+    rng = np.random.default_rng(5)
+    sig = np.array([0.3, 0.5, 1.0, 1.5] * 12)
+    w = np.stack([(s * workload.normal(7000 + k, 97)).astype(np.float32) for k, s in enumerate(sig)])
+    seeds = rng.integers(0, 2**63, 6, dtype=np.uint64)
+    sc, pc, lc = ev.eval_full(w, w.shape[0], seeds, 150)
+    osc, opc, olc, _ = oracle_eval(oracle, w, seeds, 150)
+    assert sc.tobytes() == osc.tobytes()
+    assert np.array_equal(pc, opc) and np.array_equal(lc, olc)
+
+
+def test_islands_equal_separate_calls(ev):
+    from tetris_ai3_b200 import workload
+    b = workload.config1(islands=3, pop=4, games=5, max_moves=120, seed=9)
+    sc, pc, lc = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    for i in range(3):
+        s2, p2, l2 = ev.eval_full(b.weights[i * 4:(i + 1) * 4], 4, b.seeds[i], b.max_moves)
+        assert sc[i * 20:(i + 1) * 20].tobytes() == s2.tobytes()
+        assert np.array_equal(pc[i * 20:(i + 1) * 20], p2) and np.array_equal(lc[i * 20:(i + 1) * 20], l2)
+
+
+def test_edge_cases(ev):
+    from tetris_ai3_b200 import EvaluatorError, workload
+    w = (0.5 * workload.normal(1, 97)).astype(np.float32)
+    # max_moves = 0: no piece placed -> -1e6 (model_eval_host.cpp:51)
+    sc, pc, lc = ev.eval_full(w, 1, np.array([3, 4], np.uint64), 0)
+    assert sc.tolist() == [-1.0e6, -1.0e6] and pc.tolist() == [0, 0]
+    # empty batches
+    assert ev.eval_full(w[:0], 0, np.array([1], np.uint64), 10)[0].size == 0
+    assert ev.eval_full(w, 1, np.array([], np.uint64), 10)[0].size == 0
+    # parameter-count mismatch raises (model_eval.cu:110-111)
+    with pytest.raises(EvaluatorError):
+        ev.eval(np.zeros(96, np.float32), 1, np.array([1], np.uint64), 5)
+    # extreme seeds and a single move
+    seeds = np.array([0, 2**64 - 1, 2**63], np.uint64)
+    sc, pc, lc = ev.eval_full(w, 1, seeds, 1)
+    assert pc.tolist() == [1, 1, 1]
+
+
+def test_extreme_weights_match_oracle(ev, oracle):
+    # all-zero weights (every value ties at +0: tie-breaks decide everything), huge and tiny magnitudes
+    from tetris_ai3_b200 import workload
+    w = np.stack([np.zeros(97, np.float32),
+                  (300.0 * workload.normal(11, 97)).astype(np.float32),
+                  (1e-3 * workload.normal(12, 97)).astype(np.float32),
+                  np.where(workload.normal(13, 97) > 0, 1.0, -1.0).astype(np.float32)])
+    seeds = np.array([5, 6, 7], np.uint64)
+    sc, pc, lc = ev.eval_full(w, 4, seeds, 120)
+    osc, opc, olc, _ = oracle_eval(oracle, w, seeds, 120)
+    assert sc.tobytes() == osc.tobytes() and np.array_equal(pc, opc) and np.array_equal(lc, olc)
+
+
+def test_full_config1_properties(ev, oracle):
+    # configs[1] at full size: deterministic, island-consistent, and a sample matches the oracle
+    from tetris_ai3_b200 import workload
+    b = workload.config1()
+    sc1, pc1, lc1 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    sc2, pc2, lc2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    assert sc1.tobytes() == sc2.tobytes() and np.array_equal(pc1, pc2)
+    assert (pc1 <= b.max_moves).all() and (lc1 <= 4 * pc1).all()
+    # sample: the shortest 24 sims of island 0 replayed by the oracle
+    idx = np.argsort(pc1[:50 * 50], kind="stable")[:24]
+    for i in idx:
+        m, g = divmod(int(i), 50)
+        osc, opc, olc, _ = oracle_eval(oracle, b.weights[m], b.seeds[0][g:g + 1], b.max_moves, threads=1)
+        assert osc[0].tobytes() == sc1[i].tobytes() and opc[0] == pc1[i] and olc[0] == lc1[i]

@@ -1,0 +1,172 @@
+"""Python host mirror of the reference evaluator seam, over the C ABI in
+include/ta3b.h (tetris_ai3_b200/_lib/libta3b.so).
+
+``ModelEvaluator`` mirrors ``ta3::gpu::ModelEvaluator``
+(ta3_gpu/incl/ta3/gpu/model_eval.hpp:27-77) and ``simulate`` mirrors
+``ta3::gpu::simulate`` (model_eval.hpp:84-114): same argument meaning,
+model-major outputs, and a raised exception where the reference throws
+``std::runtime_error``. There is no CPU fallback: without the CUDA library or
+a B200 the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .workload import NUM_PARAMS
+
+_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libta3b.so")
+_lib = None
+
+EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
+           "ta3b_eval_trace", "ta3b_simulate_seeds", "ta3b_launch_info"]
+
+
+class EvaluatorError(RuntimeError):
+    """A failed evaluator call (the reference raises std::runtime_error)."""
+
+
+class _Config(C.Structure):
+    _fields_ = [("device", C.c_int), ("warps_per_block", C.c_uint32), ("blocks_per_sm", C.c_uint32)]
+
+
+def library(path: str | None = None) -> C.CDLL:
+    """Load the C-ABI library; raises if it was not built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or _LIB_PATH
+    if not os.path.exists(p):
+        raise EvaluatorError(f"CUDA evaluator library missing: {p} (run python -m tetris_ai3_b200.build)")
+    lib = C.CDLL(p)
+    vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+    lib.ta3b_create.restype = vp
+    lib.ta3b_create.argtypes = [C.POINTER(_Config)]
+    lib.ta3b_destroy.argtypes = [vp]
+    lib.ta3b_last_error.restype = C.c_char_p
+    lib.ta3b_last_error.argtypes = [vp]
+    lib.ta3b_eval.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp]
+    lib.ta3b_eval_islands.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp]
+    lib.ta3b_eval_device.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp]
+    lib.ta3b_eval_trace.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp]
+    lib.ta3b_simulate_seeds.argtypes = [u64, u32, vp]
+    lib.ta3b_launch_info.argtypes = [vp, vp, vp, vp]
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def simulate_seeds(seed: int, games: int) -> np.ndarray:
+    out = np.zeros(games, np.uint64)
+    rc = library().ta3b_simulate_seeds(C.c_uint64(seed & (2**64 - 1)), games, _p(out))
+    if rc:
+        raise EvaluatorError("ta3b_simulate_seeds failed")
+    return out
+
+
+class ModelEvaluator:
+    """One evaluation context: a CUDA stream plus grow-only device buffers.
+    Not thread-safe; use one instance per host thread."""
+
+    def __init__(self, device: int = 0, warps_per_block: int = 0, blocks_per_sm: int = 0):
+        self._lib = library()
+        cfg = _Config(device, warps_per_block, blocks_per_sm)
+        self._ctx = self._lib.ta3b_create(C.byref(cfg))
+        if not self._ctx:
+            raise EvaluatorError(self._lib.ta3b_last_error(None).decode())
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.ta3b_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, rc: int):
+        if rc != 0:
+            raise EvaluatorError(self._lib.ta3b_last_error(self._ctx).decode())
+
+    @staticmethod
+    def _prep(weights, num_models, seeds):
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
+        s = np.ascontiguousarray(seeds, dtype=np.uint64).reshape(-1)
+        if w.size != num_models * NUM_PARAMS:
+            raise EvaluatorError("weights.size() must equal num_models * NUM_PARAMS")
+        return w, s
+
+    def eval(self, weights, num_models: int, seeds, max_moves: int) -> np.ndarray:
+        """Per-(model, game) fitness, model-major (index m * len(seeds) + g)."""
+        return self.eval_full(weights, num_models, seeds, max_moves)[0]
+
+    def eval_full(self, weights, num_models: int, seeds, max_moves: int):
+        """(score, pieces, lines), each model-major."""
+        w, s = self._prep(weights, num_models, seeds)
+        n = num_models * s.size
+        sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        self._check(self._lib.ta3b_eval(self._ctx, _p(w), num_models, NUM_PARAMS, _p(s), s.size, max_moves, _p(sc),
+                                        _p(pc), _p(lc)))
+        return sc, pc, lc
+
+    def eval_islands(self, weights, seeds_per_island, max_moves: int):
+        """weights (islands * models_per_island, 97); seeds_per_island (islands, games)."""
+        s = np.ascontiguousarray(seeds_per_island, dtype=np.uint64)
+        islands, games = s.shape
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1, NUM_PARAMS)
+        if w.shape[0] % islands:
+            raise EvaluatorError("model count must be a multiple of the island count")
+        mpi = w.shape[0] // islands
+        n = w.shape[0] * games
+        sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        self._check(self._lib.ta3b_eval_islands(self._ctx, _p(w), islands, mpi, NUM_PARAMS, _p(s), games, max_moves,
+                                                _p(sc), _p(pc), _p(lc)))
+        return sc, pc, lc
+
+    def eval_trace(self, weights, num_models: int, seeds, max_moves: int):
+        """Everything, plus per-move traces: dict of model-major arrays."""
+        w, s = self._prep(weights, num_models, seeds)
+        n = num_models * s.size
+        out = {"score": np.zeros(n, np.float32), "pieces": np.zeros(n, np.uint32), "lines": np.zeros(n, np.uint32),
+               "evals": np.zeros(n, np.uint32), "trace": np.zeros((n, max(max_moves, 1) * 3), np.uint8),
+               "moves": np.zeros(n, np.uint32), "board": np.zeros((n, 10), np.uint32)}
+        self._check(self._lib.ta3b_eval_trace(self._ctx, _p(w), num_models, NUM_PARAMS, _p(s), s.size, max_moves,
+                                              _p(out["score"]), _p(out["pieces"]), _p(out["lines"]),
+                                              _p(out["evals"]), _p(out["trace"]), _p(out["moves"]),
+                                              _p(out["board"])))
+        return out
+
+    def eval_device(self, weights, seeds, max_moves: int, score, pieces=None, lines=None, evals=None,
+                    num_islands: int = 1, stream=None):
+        """Device-resident batch (torch CUDA tensors); enqueued, not synchronised.
+        weights (islands * mpi, 97) float32, seeds (islands, games) uint64 viewed as int64."""
+        islands = num_islands
+        games = seeds.numel() // islands
+        models = weights.numel() // NUM_PARAMS
+        ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
+        st = C.c_void_p(stream.cuda_stream) if stream is not None else None
+        self._check(self._lib.ta3b_eval_device(self._ctx, ptr(weights), islands, models // islands, NUM_PARAMS,
+                                               ptr(seeds), games, max_moves, ptr(score), ptr(pieces), ptr(lines),
+                                               ptr(evals), st))
+
+    def launch_info(self):
+        g, w, s = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        self._check(self._lib.ta3b_launch_info(self._ctx, C.byref(g), C.byref(w), C.byref(s)))
+        return {"grid": g.value, "warps_per_block": w.value, "sms": s.value}
+
+
+def simulate(evaluator: ModelEvaluator, model_weights, num_models: int, games: int, seed: int,
+             max_moves: int) -> np.ndarray:
+    """ta3::gpu::simulate: games seeds drawn from xoshiro256**(seed), shared by every model."""
+    return evaluator.eval(model_weights, num_models, simulate_seeds(seed, games), max_moves)
