@@ -197,7 +197,7 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     # weak scaling: each rank scores its own generation (islands seeded per rank)
-    batch = workload.config1(seed=1 + rank)
+    batch = workload.config1(islands=args.islands, pop=args.pop, games=args.games, max_moves=args.cap, seed=1 + rank)
     ev = ModelEvaluator(device=local)
     stream = torch.cuda.Stream(device=dev)
     w_dev = torch.from_numpy(batch.weights).to(dev)
@@ -214,6 +214,11 @@ def run_ours(args):
         ev.eval_device(w_dev, s_dev, batch.max_moves, score, pieces, lines, evals, num_islands=batch.islands,
                        stream=stream)
 
+    tune = None
+    if args.variant >= 0:
+        ev.select_variant(args.variant)
+    elif not args.no_autotune:
+        tune = ev.autotune(w_dev, s_dev, batch.max_moves, score, pieces, lines, evals, batch.islands, stream)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             step()
@@ -304,7 +309,8 @@ def run_ours(args):
                 "config": {"workload": batch.name, "global_batch": batch.sims * world, "seq_len": batch.max_moves,
                            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                            "l2": "flushed (256 MB write) between timed steps",
-                           "launch": ev.launch_info()},
+                           "launch": ev.launch_info(),
+                           "autotune_ms": tune},
                 "sims_per_step": batch.sims, "placements_per_step": total_pl / args.steps / world,
                 "clocks": clocks, "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -325,6 +331,13 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--ref-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=-1, help="fixed kernel variant (default: autotune)")
+    ap.add_argument("--no-autotune", action="store_true")
+    # reduced shapes for profiling captures only (the headline is the default configs[1])
+    ap.add_argument("--islands", type=int, default=4)
+    ap.add_argument("--pop", type=int, default=50)
+    ap.add_argument("--games", type=int, default=50)
+    ap.add_argument("--cap", type=int, default=2000)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

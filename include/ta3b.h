@@ -40,8 +40,8 @@ typedef struct ta3b_ctx ta3b_ctx;
 
 typedef struct {
     int device;                /* CUDA device ordinal */
-    uint32_t warps_per_block;  /* 0 = tuned default */
-    uint32_t blocks_per_sm;    /* 0 = as many as fit */
+    uint32_t warps_per_block;  /* 0 = tuned default; else pick the kernel variant with this shape */
+    uint32_t blocks_per_sm;    /* 0 = tuned default; else the variant's minimum resident blocks per SM */
 } ta3b_config;
 
 /* Create an evaluation context (stream + grow-only device buffers).
@@ -95,9 +95,35 @@ int ta3b_eval_trace(ta3b_ctx* ctx, const float* weights, uint32_t num_models, ui
                     float* score_out, uint32_t* pieces_out, uint32_t* lines_out, uint32_t* evals_out,
                     uint8_t* trace_out, uint32_t* n_moves_out, uint32_t* board_out);
 
+/* Scheduling profile of one island-batched evaluation (tooling): like
+ * ta3b_eval_islands plus, per sim, the number of evaluated placements and the
+ * device global-timer (ns) at which a warp started and finished it
+ * (timing_out: 2 values per sim). No reference counterpart. */
+int ta3b_eval_timed(ta3b_ctx* ctx, const float* weights, uint32_t num_islands, uint32_t models_per_island,
+                    uint32_t num_params, const uint64_t* seeds, uint32_t num_games, uint32_t max_moves,
+                    float* score_out, uint32_t* pieces_out, uint32_t* evals_out, uint64_t* timing_out);
+
 /* The seeds ta3::gpu::simulate derives for `games` games from one seed
  * (xoshiro256** draws), ta3_gpu/incl/ta3/gpu/model_eval.hpp:84-103. Host only. */
 int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out);
+
+/* Kernel launch-shape variants (warps per block x register cap expressed as
+ * minimum resident blocks per SM): the autotuner's search space. No reference
+ * counterpart (the reference has one fixed launch, model_eval.cu:143). */
+int ta3b_num_variants(void);
+int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm);
+int ta3b_select_variant(ta3b_ctx* ctx, int variant);
+
+/* Device self-test of the per-candidate evaluation (tests and tooling): one
+ * thread per candidate runs the incremental fast path and the full reference
+ * path on caller-built parent records (80 words each, the layout of
+ * tetris_ai3_b200/csrc/eval_core.h). cand[t] = piece | placement << 8 |
+ * held-is-I << 16 | record index << 17. Outputs per candidate: fast status
+ * (0 evaluated, 1 deferred) and value, full-path legality and value; dbg32
+ * (may be NULL) receives 32 diagnostic floats per candidate from the fast path.
+ * No reference counterpart. */
+int ta3b_core_selftest(const uint32_t* recs, uint32_t num_recs, const uint32_t* cand, uint32_t n, const float* w97,
+                       float* fast_v, int* fast_st, float* full_v, int* full_legal, float* dbg32);
 
 /* Launch shape the context uses (after the first evaluation): grid blocks,
  * warps per block, sims per launch. For tooling and the autotuner. */

@@ -131,3 +131,51 @@ def test_full_config1_properties(ev, oracle):
         m, g = divmod(int(i), 50)
         osc, opc, olc, _ = oracle_eval(oracle, b.weights[m], b.seeds[0][g:g + 1], b.max_moves, threads=1)
         assert osc[0].tobytes() == sc1[i].tobytes() and opc[0] == pc1[i] and olc[0] == lc1[i]
+
+
+def test_device_core_matches_host_core(ev):
+    """The per-candidate core on the device (fast and full path, one thread per
+    candidate) equals the host build of the same code on random records."""
+    import ctypes as C
+    from tetris_ai3_b200 import build, library, workload
+    from test_core_host import boards, NPLACE
+    from conftest import ptr
+    host = C.CDLL(build.CORETEST_LIB) if __import__("os").path.exists(build.CORETEST_LIB) else \
+        C.CDLL(build.build_coretest())
+    rng = np.random.default_rng(3)
+    w = (0.5 * workload.normal(77, 97)).astype(np.float32)
+    bds = [b for b in boards(rng, 120) if not (int(np.bitwise_and.reduce(b)) & ((1 << 23) - 1))]
+    recs = np.zeros((len(bds), 80), np.uint32)
+    for k, b in enumerate(bds):
+        clears = int(rng.integers(0, 3)) | (int(rng.integers(0, 2)) << 16)
+        host.ta3bt_build_record(ptr(b), C.c_uint32(clears), ptr(w), ptr(recs[k]))
+    cand = np.array([p | (i << 8) | (int(rng.integers(0, 2)) << 16) | (k << 17)
+                     for k in range(len(bds)) for p in range(7) for i in range(NPLACE[p])], np.uint32)
+    n = cand.size
+    fv, fs, uv, ul = np.zeros(n, np.float32), np.zeros(n, np.int32), np.zeros(n, np.float32), np.zeros(n, np.int32)
+    dd = np.zeros((n, 32), np.float32)
+    assert library().ta3b_core_selftest(ptr(recs), len(bds), ptr(cand), n, ptr(w), ptr(fv), ptr(fs), ptr(uv),
+                                        ptr(ul), ptr(dd)) == 0
+    hv, hs = C.c_float(), None
+    hd = np.zeros(32, np.float32)
+    mism = []
+    for t in range(n):
+        c = int(cand[t])
+        p, i, held, k = c & 0xFF, (c >> 8) & 0xFF, (c >> 16) & 1, c >> 17
+        hd[:] = 0
+        st = host.ta3bt_fast(ptr(recs[k]), p, i, held, ptr(w), C.byref(hv), ptr(hd))
+        if st != fs[t] or (st == 0 and np.float32(hv.value).tobytes() != fv[t].tobytes()):
+            diff = [j for j in range(18) if hd[j].tobytes() != dd[t][j].tobytes()]
+            mism.append(("fast", t, p, i, st, int(fs[t]), hv.value, float(fv[t]), "first differing diag",
+                         diff[:3], [float(hd[j]) for j in diff[:3]], [float(dd[t][j]) for j in diff[:3]]))
+        v2, cl, out = C.c_float(), C.c_uint32(), np.zeros(10, np.uint32)
+        lg = host.ta3bt_full(ptr(recs[k][8:18].copy()), C.c_uint32(int(recs[k][18])), p, i, held, ptr(w),
+                             C.byref(v2), C.byref(cl), ptr(out))
+        if lg != ul[t] or (lg and np.float32(v2.value).tobytes() != uv[t].tobytes()):
+            mism.append(("full", t, p, i, lg, int(ul[t]), v2.value, float(uv[t])))
+    for m in mism[:8]:
+        print("MISMATCH", m)
+    # the packed PTX f32x2 arithmetic (diagnostic slot 31) must give the same bits where the path evaluates
+    packed_bad = int(((fs == 0) & (dd[:, 31].view(np.uint32) != fv.view(np.uint32))).sum())
+    print("packed f32x2 MLP mismatches:", packed_bad, "of", int((fs == 0).sum()))
+    assert not mism, f"{len(mism)} of {n} candidates differ"

@@ -49,6 +49,19 @@ def build_lib(verbose: bool = False) -> str:
     return res.stderr
 
 
+CORETEST_LIB = os.path.join(LIBDIR, "libta3b_coretest.so")
+
+
+def build_coretest() -> str:
+    """Host build of csrc/eval_core.h for the CPU tests (never loaded by the product)."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-std=c++20", "-O2", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", "-I", CSRC,
+           "-o", CORETEST_LIB, os.path.join(CSRC, "core_selftest.cpp")]
+    subprocess.run(cmd, check=True)
+    return CORETEST_LIB
+
+
 def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
 
@@ -65,6 +78,7 @@ def build_reference_cpu() -> bool:
 
 if __name__ == "__main__":
     log = build_lib(verbose=True)
+    build_coretest()
     build_oracle()
     build_reference_cpu()
     print("built", LIB)

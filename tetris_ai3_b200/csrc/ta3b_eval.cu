@@ -10,15 +10,18 @@
 //   mid level 1   <= 1088           -> top 32          (beam.hpp:337-403)
 //   mid level 2   <= 2176           -> top 32
 //   leaf stage    <= 2176           -> argmax key      (beam.hpp:407-443)
-// Lanes stride the flattened (parent, child list, placement) space of a level;
-// every candidate is one fused apply (fit + lock + line clear) + v11 features
-// + FP32 MLP, evaluated in the reference's operation order. The top-K of a
-// level is a warp-distributed sorted list (lane i holds the i-th best packed
-// key) maintained with ballots and shuffles, so level scores never touch
-// memory. Kept frontier boards live in per-warp shared memory; nothing in the
-// move loop synchronises more than one warp.
+// Lanes stride the flattened (parent, child list, placement) space of a level.
+// Each kept frontier node gets a parent record in shared memory (heights,
+// holes, row fills, feature totals, hidden-layer partial sums; eval_core.h),
+// so a candidate is evaluated incrementally from the <= 4 columns it touches;
+// candidates that clear a row or reach into the spawn rows are queued and
+// evaluated by the full reference algorithm in compacted 32-lane batches.
+// The top-K of a level is a warp-distributed sorted list (lane i holds the
+// i-th best packed key) maintained with ballots and shuffles, so level scores
+// never touch memory. Nothing in the move loop synchronises more than one warp.
 #include "ta3b.h"
 #include "tables.h"
+#include "eval_core.h"
 
 #include <cuda_runtime.h>
 
@@ -30,16 +33,10 @@ namespace ta3b {
 namespace {
 
 constexpr int WARP = 32;
+constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
 
 // ---------------------------------------------------------------- tables ---
-// Placement LUT packed one u32 per placement: cols (16) | col0 (4) << 16 |
-// orientation (2) << 20 | (x + 2) (4) << 24.
-__host__ __device__ constexpr uint32_t pack_place(Place p) {
-    return uint32_t(p.cols) | (uint32_t(p.col0) << 16) | (uint32_t(p.orient) << 20) | (uint32_t(p.x + 2) << 24);
-}
-
 struct DevTables {
-    uint32_t place[NPIECE][MP];
     uint32_t nplace[NPIECE];
     uint32_t spawn_cols[NPIECE];
     uint32_t spawn_col0[NPIECE];
@@ -52,7 +49,6 @@ struct DevTables {
 constexpr DevTables make_dev_tables() {
     DevTables d{};
     for (int p = 0; p < NPIECE; ++p) {
-        for (int i = 0; i < MP; ++i) d.place[p][i] = i < TABLES.nplace[p] ? pack_place(TABLES.place[p][i]) : 0u;
         d.nplace[p] = TABLES.nplace[p];
         d.spawn_cols[p] = TABLES.spawn_cols[p];
         d.spawn_col0[p] = uint32_t(TABLES.spawn_col0[p]);
@@ -72,29 +68,28 @@ constexpr DevTables make_dev_tables() {
 
 __constant__ DevTables c_tables = make_dev_tables();
 
-// ------------------------------------------------------------ bit helpers ---
-__device__ __forceinline__ int ctz32(uint32_t v) { return __ffs(int(v)) - 1; }   // v != 0
-__device__ __forceinline__ int column_top(uint32_t col) { return ctz32(col | FLOOR); }
-
-__device__ __forceinline__ uint32_t ordered_bits(float v) {                  // beam.hpp:204-207
-    uint32_t const u = __float_as_uint(v);
-    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+// Placement tables copied into shared memory per block: the incremental-path
+// data (PlaceFast) and the move itself packed as cols (16) | col0 (4) << 16 |
+// orientation (2) << 20 | (x + 2) (4) << 24.
+struct LutTables {
+    PlaceFast fast[NPIECE][MP];
+    uint32_t move[NPIECE][MP];
+};
+constexpr LutTables make_lut_tables() {
+    LutTables t{};
+    for (int p = 0; p < NPIECE; ++p)
+        for (int i = 0; i < TABLES.nplace[p]; ++i) {
+            Place const pl = TABLES.place[p][i];
+            t.fast[p][i] = FAST.place[p][i];
+            t.move[p][i] = uint32_t(pl.cols) | (uint32_t(pl.col0) << 16) | (uint32_t(pl.orient) << 20) |
+                           (uint32_t(pl.x + 2) << 24);
+        }
+    return t;
 }
+__device__ LutTables const g_lut = make_lut_tables();
+
 __device__ __forceinline__ float ordered_bits_inv(uint32_t s) {              // beam.hpp:209-211
     return __uint_as_float((s & 0x80000000u) ? (s ^ 0x80000000u) : ~s);
-}
-__device__ __forceinline__ uint32_t clear_bump(int cleared) {                // model_defs.hpp:177-183
-    return cleared == 0 ? 0u : 1u << (8 * (cleared - 1));
-}
-
-// remove the rows flagged in `full` from one column, survivors drop down (board2.hpp:218-234)
-__device__ __forceinline__ uint32_t clear_rows(uint32_t col, uint32_t full) {
-    while (full) {
-        uint32_t const row = full & (~full + 1u);
-        col = ((col & (row - 1u)) << 1) | (col & ~((row << 1) - 1u));
-        full ^= row;
-    }
-    return col;
 }
 
 // ------------------------------------------------------------ game state ---
@@ -189,128 +184,26 @@ __device__ int engine_place(Engine& e, int o, int x) {                       // 
     uint32_t const p = e.queue[0];
     uint32_t const cols = c_tables.shape_cols[p][o];
     int const col0 = x + c_tables.shape_left[p][o];
-    int drop = H;
-    for (int i = 0; i < 4; ++i) {                                            // board2.hpp:262-275
-        uint32_t const nib = (cols >> (4 * i)) & 0xFu;
-        if (nib == 0) continue;
-        int const low = 31 - __clz(nib);
-        int const d = column_top(e.board[col0 + i] & ~((2u << low) - 1u)) - low - 1;
-        drop = d < drop ? d : drop;
-    }
-    uint32_t full = FIELD;
-    for (int i = 0; i < 4; ++i) {
-        uint32_t const nib = (cols >> (4 * i)) & 0xFu;
-        if (nib) e.board[col0 + i] |= nib << drop;
-    }
-    for (int c = 0; c < W; ++c) full &= e.board[c];
-    int const cleared = __popc(full);
-    if (full)
-        for (int c = 0; c < W; ++c) e.board[c] = clear_rows(e.board[c], full);
+    uint32_t b[W], nb[W];
+    for (int c = 0; c < W; ++c) b[c] = e.board[c];
+    int cleared = 0;
+    // the search only commits legal moves, so this is the drop + lock + clear of board2.hpp
+    apply_full(b, cols, col0, nb, cleared);
+    for (int c = 0; c < W; ++c) e.board[c] = nb[c];
     advance_queue(e);
     update_game_over(e);
     return e.over ? -1 : cleared;
 }
 
-// ------------------------------------------------------------ value model ---
-// Integer board metrics of ta3_ai/incl/ta3/ai/models/metrics/v_board_metrics.hpp:130-225.
-struct BoardInts {
-    uint32_t holes, hole_depths, max_height, wells;
-    int surf_sq;
+// ------------------------------------------------------------ candidates ---
+struct SmemW {                       // weights read from shared memory (broadcast loads)
+    float const* p;
+    __device__ __forceinline__ float operator()(int i) const { return p[i]; }
 };
-
-__device__ __forceinline__ BoardInts board_ints(uint32_t const (&b)[W]) {
-    BoardInts r{0, 0, 0, 0, 0};
-    int h[W];
-#pragma unroll
-    for (int x = 0; x < W; ++x) {
-        uint32_t const col = b[x];
-        h[x] = H - column_top(col);
-        int const n = __popc(col);
-        r.holes += uint32_t(h[x] - n);
-        r.max_height = max(r.max_height, uint32_t(h[x]));
-        // sum of occupied row indices via the 5 bit planes of the row index
-        int const s = __popc(col & 0x2AAAAAu) + 2 * __popc(col & 0x4CCCCCu) + 4 * __popc(col & 0x70F0F0u) +
-                      8 * __popc(col & 0x00FF00u) + 16 * __popc(col & 0x7F0000u);
-        // (H-1)n + n(n+1)/2 - (s + n^2): occupied cells' count of empty cells beneath them
-        r.hole_depths += uint32_t((H - 1) * n + n * (n + 1) / 2 - (s + n * n));
-    }
-#pragma unroll
-    for (int x = 1; x < W; ++x) {
-        int const d = h[x] - h[x - 1];
-        r.surf_sq += d * d;
-    }
-    uint32_t wells = (h[1] >= h[0] + 3) + (h[W - 2] >= h[W - 1] + 3);
-#pragma unroll
-    for (int x = 1; x < W - 1; ++x) wells += (h[x - 1] >= h[x] + 3 && h[x + 1] >= h[x] + 3);
-    r.wells = wells;
-    return r;
-}
-
-struct Model {                       // 97 v11 weights, model_v11.hpp:166-180 layout
-    float w[NPARAMS];
+struct GlobalW {
+    float const* p;
+    __device__ __forceinline__ float operator()(int i) const { return __ldg(p + i); }
 };
-
-// ModelV11::extractInputs + forward (model_v11.hpp:63-91,166-180; utility.hpp:30-46),
-// each multiply and add rounded separately in the reference order.
-__device__ __forceinline__ float evaluate(uint32_t clear_bits, uint32_t const (&b)[W], bool held_i, Model const& m) {
-    BoardInts const bi = board_ints(b);
-    float in[NIN];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) in[k] = __fmul_rn(float((clear_bits >> (8 * k)) & 0xFFu), 0.25f);
-    float const sv = bi.surf_sq > 0 ? __fsqrt_rn(float(bi.surf_sq)) : 0.0f;
-    in[4] = __fdiv_rn(sv, 100.0f);
-    in[5] = __fdiv_rn(float(bi.holes), 20.0f);
-    in[6] = __fdiv_rn(float(bi.hole_depths), 200.0f);
-    in[7] = float(bi.max_height);
-    in[8] = held_i ? 1.0f : 0.0f;
-    in[9] = __fdiv_rn(float(bi.wells), 5.0f);
-    float hid[NHID];
-#pragma unroll
-    for (int o = 0; o < NHID; ++o) {
-        float v = m.w[NIN * NHID + o];
-#pragma unroll
-        for (int i = 0; i < NIN; ++i) v = __fadd_rn(v, __fmul_rn(in[i], m.w[o * NIN + i]));
-        hid[o] = v > 0.0f ? v : 0.0f;
-    }
-    float v = m.w[NIN * NHID + NHID + NHID];
-#pragma unroll
-    for (int i = 0; i < NHID; ++i) v = __fadd_rn(v, __fmul_rn(hid[i], m.w[NIN * NHID + NHID + i]));
-    return v;
-}
-
-// ------------------------------------------------------------- candidate ---
-// search.hpp:61-70 apply(): spawn-collision + drop (board2.hpp:306-320), lock
-// (board2.hpp:322-327) and line clear (board2.hpp:333-342). Returns legality;
-// nb receives the resulting board and cleared the rows removed.
-__device__ __forceinline__ bool apply(uint32_t const (&b)[W], uint32_t pl, uint32_t (&nb)[W], int& cleared) {
-    uint32_t const cols = pl & 0xFFFFu;
-    int const col0 = int((pl >> 16) & 0xFu);
-    uint32_t hit = 0;
-    int drop = H;
-    uint32_t nib[W];
-#pragma unroll
-    for (int x = 0; x < W; ++x) {
-        uint32_t const d = uint32_t(x - col0);
-        nib[x] = d < 4u ? (cols >> (4u * d)) & 0xFu : 0u;
-        hit |= b[x] & nib[x];
-        int const low = 31 - __clz(nib[x] | 1u);
-        int const dd = column_top(b[x] & ~((2u << low) - 1u)) - low - 1;
-        drop = (nib[x] != 0u && dd < drop) ? dd : drop;
-    }
-    if (hit) return false;
-    uint32_t full = FIELD;
-#pragma unroll
-    for (int x = 0; x < W; ++x) {
-        nb[x] = b[x] | (nib[x] << drop);
-        full &= nb[x];
-    }
-    cleared = __popc(full);
-    if (full) {
-#pragma unroll
-        for (int x = 0; x < W; ++x) nb[x] = clear_rows(nb[x], full);
-    }
-    return true;
-}
 
 __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uint32_t (&b)[W]) {
     uint4 const q0 = *reinterpret_cast<uint4 const*>(src);
@@ -321,301 +214,28 @@ __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uin
     b[8] = q2.x; b[9] = q2.y;
 }
 
-// ------------------------------------------------------------------ top-K ---
-__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
-    return (uint64_t(__shfl_sync(0xFFFFFFFFu, uint32_t(v >> 32), src)) << 32) |
-           __shfl_sync(0xFFFFFFFFu, uint32_t(v), src);
-}
-__device__ __forceinline__ uint64_t shfl64_up(uint64_t v) {
-    return (uint64_t(__shfl_up_sync(0xFFFFFFFFu, uint32_t(v >> 32), 1)) << 32) |
-           __shfl_up_sync(0xFFFFFFFFu, uint32_t(v), 1);
-}
+#ifndef TA3B_MLP_MODE
+#define TA3B_MLP_MODE MLP_SCALAR
+#endif
 
-// Fold one key per lane into the warp's sorted top-K list (lane i = i-th
-// largest, 0 = empty). Keys are unique per level (the low word encodes the
-// slot), so the kept set equals beam.hpp:244-265's "max score, lowest slot on
-// ties" whatever the insertion order.
-__device__ __forceinline__ void topk_fold(uint64_t& list, uint64_t key, int k, int lane) {
-    uint64_t thr = shfl64(list, k - 1);
-    uint32_t mask = __ballot_sync(0xFFFFFFFFu, key > thr);
-    while (mask) {
-        int const s = __ffs(int(mask)) - 1;
-        uint64_t const x = shfl64(key, s);
-        int const pos = __popc(__ballot_sync(0xFFFFFFFFu, list > x));
-        uint64_t const up = shfl64_up(list);
-        if (lane > pos && lane < k) list = up;
-        if (lane == pos) list = x;
-        thr = shfl64(list, k - 1);
-        mask &= ~(1u << s);
-        mask &= __ballot_sync(0xFFFFFFFFu, key > thr);
-    }
-}
-
-__device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        uint64_t const u = shfl64(v, (threadIdx.x + o) & 31);
-        v = u > v ? u : v;
-    }
-    return v;
-}
-
-// ---------------------------------------------------------------- kernel ---
-struct alignas(16) WarpShared {
-    uint32_t fboard[32][12];          // kept frontier boards (rank -> board), 48-byte rows
-    Engine eng;                        // the committed game
-    uint32_t seg_off[65];              // per-level candidate segments (parent, child list)
-    uint32_t seg_info[64];
-    Stats st;
-};
-
-struct Params {
-    float const* weights;
-    uint64_t const* seeds;
-    float* score;
-    uint32_t* pieces;
-    uint32_t* lines;
-    uint32_t* evals;
-    uint8_t* trace;
-    uint32_t* n_moves;
-    uint32_t* board_out;
-    uint32_t* scratch;                 // [0] sim ticket, [1] error status
-    uint32_t num_games, models_per_island, max_moves, total_sims;
-};
-
-struct Move {
-    int orient, x, hold;
-    bool none;
-};
-
-// Build one level's segment table: segment j = (parent rank j/2, child j%2);
-// each spans the child piece's placement count. Returns the candidate total.
-__device__ __forceinline__ uint32_t build_segments(WarpShared& ws, uint32_t const* slot_piece, int tree, int level,
-                                                   uint32_t fnode, int kept, int lane) {
-    uint32_t base = 0;
-#pragma unroll
-    for (int half = 0; half < 2; ++half) {
-        int const j = lane + 32 * half;
-        int const k = j >> 1;
-        uint32_t const pnode = __shfl_sync(0xFFFFFFFFu, fnode, k & 31);
-        uint32_t const cnode = 2u * pnode + uint32_t(j & 1);
-        uint32_t const info = c_tables.node[tree][level][cnode & 15u];
-        uint32_t const piece = slot_piece[info & 0xFu];
-        uint32_t const held_slot = (info >> 4) & 0xFu;
-        uint32_t const held_i = held_slot != HELD_NONE && slot_piece[held_slot] == 0u;
-        uint32_t const cnt = k < kept ? c_tables.nplace[piece] : 0u;
-        // inclusive warp scan of cnt
-        uint32_t incl = cnt;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t const n = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += n;
-        }
-        ws.seg_off[j] = base + incl - cnt;
-        ws.seg_info[j] = uint32_t(k) | (piece << 8) | (held_i << 12) | (cnode << 16);
-        base += __shfl_sync(0xFFFFFFFFu, incl, 31);
-    }
-    if (lane == 0) ws.seg_off[64] = base;
-    __syncwarp();
-    return base;
-}
-
-__device__ __forceinline__ Move search_move(WarpShared& ws, Model const& m, int lane, uint32_t& evals, uint32_t* status) {
-    Move mv{0, 0, 0, true};
-    if (ws.eng.over) return mv;
-    uint32_t slot_piece[NSLOTS];                                  // beam.hpp:226-237
-    slot_piece[0] = ws.eng.held;
-    slot_piece[1] = ws.eng.queue[0];
-#pragma unroll
-    for (int i = 0; i < DEPTH; ++i) slot_piece[2 + i] = ws.eng.queue[1 + i];
-    int const tree = ws.eng.held == NO_PIECE ? 1 : 0;
-
-    // ---- root stage: score every legal root, keep the best K0 (beam.hpp:283-301,507-513)
-    uint32_t const r0 = c_tables.node[tree][0][0], r1 = c_tables.node[tree][0][1];
-    uint32_t const p0 = slot_piece[r0 & 0xFu], p1 = slot_piece[r1 & 0xFu];
-    uint32_t const h0 = (r0 >> 4) & 0xFu, h1 = (r1 >> 4) & 0xFu;
-    bool const hi0 = h0 != HELD_NONE && slot_piece[h0] == 0u;
-    bool const hi1 = h1 != HELD_NONE && slot_piece[h1] == 0u;
-    uint32_t const n0 = c_tables.nplace[p0], ntot = n0 + c_tables.nplace[p1];
-    uint32_t root_board[W];
-    load_board(ws.eng.board, root_board);
-    uint64_t list = 0;
-    for (uint32_t c0 = 0; c0 < ntot; c0 += WARP) {
-        uint32_t const c = c0 + uint32_t(lane);
-        uint64_t key = 0;
-        if (c < ntot) {
-            bool const g = c >= n0;
-            uint32_t const i = g ? c - n0 : c;
-            uint32_t const pl = c_tables.place[g ? p1 : p0][i];
-            uint32_t nb[W];
-            int cl;
-            if (apply(root_board, pl, nb, cl)) {
-                ++evals;
-                float const v = evaluate(clear_bump(cl), nb, g ? hi1 : hi0, m);
-                uint32_t const slot = (g ? MP : 0u) + i;
-                key = (uint64_t(ordered_bits(v)) << 32) | uint64_t(0xFFFFFFFFu - slot);
-            }
-        }
-        topk_fold(list, key, K0, lane);
-    }
-    int kept = __popc(__ballot_sync(0xFFFFFFFFu, list != 0));
-    if (kept == 0) return mv;                                     // no legal root: game over
-
-    // ---- seed the frontier (beam.hpp:307-329): lane k = rank k
-    uint32_t const root_slot = 0xFFFFFFFFu - uint32_t(list);      // lanes < kept
-    uint32_t fclears = 0, fscore = uint32_t(list >> 32), fnode = 0, frank = uint32_t(lane);
-    if (lane < kept) {
-        uint32_t const g = root_slot / MP;
-        uint32_t const pl = c_tables.place[g ? p1 : p0][root_slot % MP];
-        uint32_t nb[W];
-        int cl = 0;
-        apply(root_board, pl, nb, cl);
-        fclears = clear_bump(cl);
-        fnode = g;
-#pragma unroll
-        for (int x = 0; x < W; ++x) ws.fboard[lane][x] = nb[x];
-    }
-    __syncwarp();
-
-    uint64_t best = 0;                                            // leaf-order (score | order) maximum
-    // ---- middle levels (beam.hpp:540-564)
-#pragma unroll 1
-    for (int level = 1; level + 1 < DEPTH; ++level) {
-        int const kl = level == 1 ? K1 : K2;
-        uint32_t const total = build_segments(ws, slot_piece, tree, level, fnode, kept, lane);
-        uint64_t klist = 0;
-        uint32_t has_child = 0;
-        int seg = 0;
-        for (uint32_t c0 = 0; c0 < total; c0 += WARP) {
-            uint32_t const c = c0 + uint32_t(lane);
-            uint64_t key = 0;
-            uint32_t info = 0, i = 0;
-            if (c < total) {
-                while (ws.seg_off[seg + 1] <= c) ++seg;
-                info = ws.seg_info[seg];
-                i = c - ws.seg_off[seg];
-            }
-            uint32_t const k = info & 0xFFu;
-            uint32_t const pclears = __shfl_sync(0xFFFFFFFFu, fclears, int(k));
-            if (c < total) {
-                uint32_t b[W];
-                load_board(ws.fboard[k], b);
-                uint32_t const pl = c_tables.place[(info >> 8) & 0xFu][i];
-                uint32_t nb[W];
-                int cl;
-                if (apply(b, pl, nb, cl)) {
-                    ++evals;
-                    has_child |= 1u << k;
-                    float const v = evaluate(pclears + clear_bump(cl), nb, (info >> 12) & 1u, m);
-                    uint32_t const slot = (k * 2u + (uint32_t(seg) & 1u)) * MP + i;
-                    key = (uint64_t(ordered_bits(v)) << 32) | uint64_t(0xFFFFFFFFu - slot);
-                }
-            }
-            topk_fold(klist, key, kl, lane);
-        }
-        has_child = __reduce_or_sync(0xFFFFFFFFu, has_child);
-        // kept nodes with no legal continuation become leaves at this depth (beam.hpp:549-551)
-        if (lane < kept && !((has_child >> lane) & 1u)) {
-            uint64_t const fk = (uint64_t(fscore) << 32) | uint64_t(ORDER_SPAN - (LEAF_ORDERS + frank));
-            best = fk > best ? fk : best;
-        }
-        int const next = __popc(__ballot_sync(0xFFFFFFFFu, klist != 0));
-        // advance the frontier (beam.hpp:379-403): lane j builds kept node j
-        uint32_t const sslot = 0xFFFFFFFFu - uint32_t(klist);
-        uint32_t const pk = next > lane ? sslot / (2 * MP) : 0u;
-        uint32_t const child = (sslot / MP) & 1u;
-        uint32_t const par_clears = __shfl_sync(0xFFFFFFFFu, fclears, int(pk));
-        uint32_t const par_node = __shfl_sync(0xFFFFFFFFu, fnode, int(pk));
-        uint32_t const par_rank = __shfl_sync(0xFFFFFFFFu, frank, int(pk));
-        uint32_t nb[W];
-        uint32_t ncl = 0, nnode = 0;
-        if (lane < next) {
-            uint32_t const cnode = 2u * par_node + child;
-            uint32_t const piece = slot_piece[c_tables.node[tree][level][cnode] & 0xFu];
-            uint32_t b[W];
-            load_board(ws.fboard[pk], b);
-            int cl = 0;
-            apply(b, c_tables.place[piece][sslot % MP], nb, cl);
-            ncl = par_clears + clear_bump(cl);
-            nnode = cnode;
-        }
-        __syncwarp();
-        if (lane < next) {
-#pragma unroll
-            for (int x = 0; x < W; ++x) ws.fboard[lane][x] = nb[x];
-        }
-        __syncwarp();
-        fclears = ncl;
-        fscore = uint32_t(klist >> 32);
-        fnode = nnode;
-        frank = par_rank;
-        kept = next;
-    }
-
-    // ---- leaf stage (beam.hpp:407-443): argmax over leaves and per-list fallbacks
-    {
-        uint32_t const total = build_segments(ws, slot_piece, tree, DEPTH - 1, fnode, kept, lane);
-        uint32_t legal_lo = 0, legal_hi = 0;
-        int seg = 0;
-        for (uint32_t c0 = 0; c0 < total; c0 += WARP) {
-            uint32_t const c = c0 + uint32_t(lane);
-            uint32_t info = 0, i = 0;
-            if (c < total) {
-                while (ws.seg_off[seg + 1] <= c) ++seg;
-                info = ws.seg_info[seg];
-                i = c - ws.seg_off[seg];
-            }
-            uint32_t const k = info & 0xFFu;
-            uint32_t const pclears = __shfl_sync(0xFFFFFFFFu, fclears, int(k));
-            if (c < total) {
-                uint32_t b[W];
-                load_board(ws.fboard[k], b);
-                uint32_t const pl = c_tables.place[(info >> 8) & 0xFu][i];
-                uint32_t nb[W];
-                int cl;
-                if (apply(b, pl, nb, cl)) {
-                    ++evals;
-                    if (seg < 32) legal_lo |= 1u << seg;
-                    else legal_hi |= 1u << (seg - 32);
-                    float const v = evaluate(pclears + clear_bump(cl), nb, (info >> 12) & 1u, m);
-                    uint32_t const order = (k * 2u + (uint32_t(seg) & 1u)) * MP + i;
-                    uint64_t const key = (uint64_t(ordered_bits(v)) << 32) | uint64_t(ORDER_SPAN - order);
-                    best = key > best ? key : best;
-                }
-            }
-        }
-        legal_lo = __reduce_or_sync(0xFFFFFFFFu, legal_lo);
-        legal_hi = __reduce_or_sync(0xFFFFFFFFu, legal_hi);
-        // a list whose piece never fit: the frontier board is the leaf (beam.hpp:439-440)
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            int const j = lane + 32 * half;
-            int const k = j >> 1;
-            uint32_t const sc = __shfl_sync(0xFFFFFFFFu, fscore, k & 31);
-            bool const legal = ((half ? legal_hi : legal_lo) >> lane) & 1u;
-            if (k < kept && !legal) {
-                uint64_t const key = (uint64_t(sc) << 32) | uint64_t(ORDER_SPAN - uint32_t(j) * MP);
-                best = key > best ? key : best;
-            }
-        }
-    }
-    best = warp_max64(best);
-    if (best == 0) {                                              // unreachable with >= 1 root
-        if (lane == 0) atomicOr(status, 1u);
-        return mv;
-    }
-    // ---- decode the winning key back to its root move (beam.hpp:450-470)
-    uint32_t const order = ORDER_SPAN - uint32_t(best);
-    uint32_t const leaf_rank = __shfl_sync(0xFFFFFFFFu, frank, int((order / (2 * MP)) & 31u));
-    uint32_t const rank = order >= uint32_t(LEAF_ORDERS) ? order - LEAF_ORDERS : leaf_rank;
-    uint32_t const rs = __shfl_sync(0xFFFFFFFFu, root_slot, int(rank & 31u));
-    uint32_t const g = rs / MP;
-    uint32_t const pl = c_tables.place[g ? p1 : p0][rs % MP];
-    mv.orient = int((pl >> 20) & 3u);
-    mv.x = int((pl >> 24) & 0xFu) - 2;
-    mv.hold = int((c_tables.node[tree][0][g] >> 8) & 1u);
-    mv.none = ordered_bits_inv(uint32_t(best >> 32)) == -__int_as_float(0x7f800000);   // search.hpp:41
-    return mv;
+// fast path: read the parent-record words this placement needs, then eval_core's fast_eval
+template <int MLP = TA3B_MLP_MODE>
+__device__ __forceinline__ int fast_candidate(uint32_t const* __restrict__ rec, PlaceFast pf, bool held_i,
+                                              FastW const& fw, float& v, float* dbg = nullptr) {
+    RecView r;
+    float4 const p0 = *reinterpret_cast<float4 const*>(rec + R_P);
+    float4 const p1 = *reinterpret_cast<float4 const*>(rec + R_P + 4);
+    r.P[0] = p0.x; r.P[1] = p0.y; r.P[2] = p0.z; r.P[3] = p0.w;
+    r.P[4] = p1.x; r.P[5] = p1.y; r.P[6] = p1.z; r.P[7] = p1.w;
+    uint4 const q = *reinterpret_cast<uint4 const*>(rec + R_HD);       // hd, rc0, rc1, rc2
+    r.hd = q.x; r.rc0 = q.y; r.rc1 = q.z; r.rc2 = q.w;
+    r.tot = rec[R_TOT];
+    uint32_t const c0 = (pf.m >> 27) & 0xFu;
+    uint2 const sp = *reinterpret_cast<uint2 const*>(rec + R_SPAN + 2 * c0);
+    r.h4 = sp.x;
+    r.hm4 = sp.y;
+    r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
+    return fast_eval<MLP>(r, pf, held_i, fw, v, dbg);
 }
 
 // stats_v4::advance (tetris_stats.hpp:19-23 with metrics.hpp:196-229)
@@ -645,23 +265,400 @@ __device__ float final_score(Stats const& st) {
     return __double2float_rn(__dadd_rn(__dadd_rn(__dadd_rn(cb, surv), -hpen), -dpen));
 }
 
-template <int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) eval_kernel(Params p) {
-    __shared__ WarpShared s_warp[WARPS];
+// ------------------------------------------------------------------ top-K ---
+__device__ __forceinline__ uint64_t shfl64(uint64_t v, int src) {
+    return (uint64_t(__shfl_sync(FULL_MASK, uint32_t(v >> 32), src)) << 32) | __shfl_sync(FULL_MASK, uint32_t(v), src);
+}
+__device__ __forceinline__ uint64_t shfl64_up(uint64_t v) {
+    return (uint64_t(__shfl_up_sync(FULL_MASK, uint32_t(v >> 32), 1)) << 32) | __shfl_up_sync(FULL_MASK, uint32_t(v), 1);
+}
+
+// Fold one key per lane into the warp's sorted top-K list (lane i = i-th
+// largest, 0 = empty). Keys are unique per level (the low word encodes the
+// slot), so the kept set equals beam.hpp:244-265's "max score, lowest slot on
+// ties" whatever the insertion order.
+__device__ __forceinline__ void topk_fold(uint64_t& list, uint64_t key, int k, int lane) {
+    uint64_t thr = shfl64(list, k - 1);
+    uint32_t mask = __ballot_sync(FULL_MASK, key > thr);
+    while (mask) {
+        int const s = __ffs(int(mask)) - 1;
+        uint64_t const x = shfl64(key, s);
+        int const pos = __popc(__ballot_sync(FULL_MASK, list > x));
+        uint64_t const up = shfl64_up(list);
+        if (lane > pos && lane < k) list = up;
+        if (lane == pos) list = x;
+        thr = shfl64(list, k - 1);
+        mask &= ~(1u << s);
+        mask &= __ballot_sync(FULL_MASK, key > thr);
+    }
+}
+
+__device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        uint64_t const u = shfl64(v, int((threadIdx.x + o) & 31u));
+        v = u > v ? u : v;
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------- kernel ---
+struct alignas(16) WarpShared {
+    uint32_t rec[33][REC_WORDS];      // kept frontier records (rank -> record); [32] = committed board
+    float wfull[NPARAMS + 3];         // the model's weights (full path, record partial sums)
+    Engine eng;                        // the committed game
+    Stats st;
+    uint32_t seg_off[65];              // a level's candidate segments (parent rank, child list)
+    uint32_t seg_info[64];             // rec (6) | rank k << 8 | piece << 16 | held-is-I << 20 | child << 21
+    uint32_t defer[64];                // queued (segment << 8 | placement) for the full path
+};
+static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte alignment");
+
+struct Params {
+    float const* weights;
+    uint64_t const* seeds;
+    float* score;
+    uint32_t* pieces;
+    uint32_t* lines;
+    uint32_t* evals;
+    uint8_t* trace;
+    uint32_t* n_moves;
+    uint32_t* board_out;
+    uint32_t* scratch;                 // [0] sim ticket, [1] error status
+    unsigned long long* timing;        // optional: per sim [start, end] global timer (ns)
+    uint32_t num_games, models_per_island, max_moves, total_sims;
+};
+
+struct Move {
+    int orient, x, hold;
+    bool none;
+};
+
+struct LevelAcc {
+    uint64_t list;                     // top-K list (STAGE_TOPK)
+    uint64_t best;                     // argmax of leaf keys and fallbacks (STAGE_LEAF)
+    uint32_t lo, hi;                   // TOPK: bit k = parent k has a legal child; LEAF: bit = list legal
+};
+
+__device__ __forceinline__ uint64_t candidate_key(bool leaf, float v, uint32_t info, uint32_t i) {
+    uint32_t const k = (info >> 8) & 31u, child = (info >> 21) & 1u;
+    uint32_t const pos = (k * 2u + child) * MP + i;                        // beam.hpp:296,360,423
+    uint32_t const low = leaf ? uint32_t(ORDER_SPAN) - pos : 0xFFFFFFFFu - pos;   // beam.hpp:217-219
+    return (uint64_t(ordered_bits(v)) << 32) | uint64_t(low);
+}
+
+struct Luts {
+    PlaceFast const (*fast)[MP];
+    uint32_t const (*move)[MP];
+};
+
+// Full path for one queued candidate (segment << 8 | placement): its key, or 0 if illegal.
+// A legal candidate's key is never 0 (its low word is a positive position).
+__device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, uint32_t entry) {
+    uint32_t const seg = entry >> 8, i = entry & 0xFFu;
+    uint32_t const info = ws->seg_info[seg];
+    uint32_t const* rec = ws->rec[info & 63u];
+    uint32_t const mv = lut.move[(info >> 16) & 7u][i];
+    uint32_t b[W], nb[W];
+    load_board(rec + R_BOARD, b);
+    int cl = 0;
+    if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return 0;
+    BoardInts const bi = board_ints(nb);
+    float const v = value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
+    return candidate_key(leaf, v, info, i);
+}
+
+// One level: every candidate of the segment table, on the fast path or queued
+// for the full path (evaluated in compacted 32-lane batches). leaf: fold into
+// the argmax key and per-list legality; otherwise into the top-kl list and
+// per-parent legality.
+__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, bool leaf, uint32_t total,
+                                               int kl, int lane, uint32_t& evals) {
+    LevelAcc acc{0, 0, 0, 0};
+    auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
+        if (key) {
+            ++evals;
+            uint32_t const bit = leaf ? seg : (info >> 8) & 31u;
+            if (bit < 32) acc.lo |= 1u << bit;
+            else acc.hi |= 1u << (bit - 32);
+        }
+    };
+    auto fold = [&](uint64_t key) {
+        if (leaf) acc.best = key > acc.best ? key : acc.best;
+        else topk_fold(acc.list, key, kl, lane);
+    };
+    auto drain = [&](uint32_t n, uint32_t queued) {
+        uint64_t key = 0;
+        if (uint32_t(lane) < n) {
+            uint32_t const entry = ws.defer[lane];
+            key = full_key(&ws, lut, leaf, entry);
+            consume(key, entry >> 8, ws.seg_info[entry >> 8]);
+        }
+        fold(key);
+        uint32_t const rem = queued - n;
+        uint32_t t = 0;
+        __syncwarp();
+        if (uint32_t(lane) < rem) t = ws.defer[n + lane];
+        __syncwarp();
+        if (uint32_t(lane) < rem) ws.defer[lane] = t;
+        __syncwarp();
+    };
+    uint32_t queued = 0;
+    int seg = 0;
+    for (uint32_t c0 = 0; c0 < total; c0 += WARP) {
+        uint32_t const c = c0 + uint32_t(lane);
+        uint64_t key = 0;
+        bool def = false;
+        uint32_t entry = 0;
+        if (c < total) {
+            while (ws.seg_off[seg + 1] <= c) ++seg;
+            uint32_t const info = ws.seg_info[seg];
+            uint32_t const i = c - ws.seg_off[seg];
+            PlaceFast const pf = lut.fast[(info >> 16) & 7u][i];
+            float v;
+            if (fast_candidate(ws.rec[info & 63u], pf, (info >> 20) & 1u, fw, v) == FAST_OK) {
+                key = candidate_key(leaf, v, info, i);
+                consume(key, uint32_t(seg), info);
+            } else {
+                def = true;
+                entry = (uint32_t(seg) << 8) | i;
+            }
+        }
+        uint32_t const dm = __ballot_sync(FULL_MASK, def);
+        if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = entry;
+        queued += __popc(dm);
+        fold(key);
+        if (queued >= uint32_t(WARP)) {
+            __syncwarp();
+            drain(WARP, queued);
+            queued -= WARP;
+        }
+    }
+    __syncwarp();
+    while (queued) {
+        uint32_t const n = queued < uint32_t(WARP) ? queued : uint32_t(WARP);
+        drain(n, queued);
+        queued -= n;
+    }
+    return acc;
+}
+
+// Segment table of one level: segment j = (parent rank j/2, child list j%2),
+// spanning the child piece's placement count. Returns the candidate total.
+__device__ __forceinline__ uint32_t build_segments(WarpShared& ws, uint32_t const* slot_piece, int tree, int level,
+                                                   uint32_t fnode, int kept, int lane) {
+    uint32_t base = 0;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        int const j = lane + 32 * half;
+        int const k = j >> 1;
+        uint32_t const pnode = __shfl_sync(FULL_MASK, fnode, k & 31);
+        uint32_t const cnode = (2u * pnode + uint32_t(j & 1)) & 15u;
+        uint32_t const nd = c_tables.node[tree][level][cnode];
+        uint32_t const piece = slot_piece[nd & 0xFu];
+        uint32_t const held_slot = (nd >> 4) & 0xFu;
+        uint32_t const held_i = held_slot != HELD_NONE && slot_piece[held_slot] == 0u;
+        uint32_t const cnt = k < kept ? c_tables.nplace[piece] : 0u;
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t const n = __shfl_up_sync(FULL_MASK, incl, o);
+            if (lane >= o) incl += n;
+        }
+        ws.seg_off[j] = base + incl - cnt;
+        ws.seg_info[j] = uint32_t(k & 31) | (uint32_t(k & 31) << 8) | (piece << 16) | (held_i << 20) |
+                         (uint32_t(j & 1) << 21);
+        base += __shfl_sync(FULL_MASK, incl, 31);
+    }
+    if (lane == 0) ws.seg_off[64] = base;
+    __syncwarp();
+    return base;
+}
+
+// lane j builds kept node j (when active): parent record `prec`, placement (piece, i)
+__device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, uint32_t prec, uint32_t piece,
+                                         uint32_t i, int lane) {
+    uint32_t nb[W];
+    uint32_t ncl = 0;
+    if (active) {
+        uint32_t const* pr = ws->rec[prec];
+        uint32_t b[W];
+        load_board(pr + R_BOARD, b);
+        uint32_t const mv = lut.move[piece][i];
+        int cl = 0;
+        apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl);
+        ncl = pr[R_CLEARS] + clear_bump(cl);
+    }
+    __syncwarp();
+    if (active) build_record(nb, ncl, SmemW{ws->wfull}, ws->rec[lane]);
+    __syncwarp();
+}
+
+// the committed board's record (record 32), built by the whole warp
+__device__ __noinline__ void root_record(WarpShared* ws, int lane) {
+    uint32_t b[W];
+    load_board(ws->eng.board, b);
+    ColumnData c;
+    column_data(b, c);
+    uint32_t* rec = ws->rec[32];
+    if (lane < W) {
+        rec[R_BOARD + lane] = b[lane];
+        span_words(c, lane, rec[R_SPAN + 2 * lane], rec[R_SPAN + 2 * lane + 1]);
+    }
+    for (int id = lane; id < NCOMBO; id += WARP) {
+        int c0, wd;
+        combo_of(id, c0, wd);
+        rec[R_COMBO + id] = combo_word(c, c0, wd);
+    }
+    if (lane < NHID) rec[R_P + lane] = partial_word(0u, lane, SmemW{ws->wfull});
+    if (lane >= 16 && lane < 19) rec[R_RC + lane - 16] = row_counts(b, lane - 16);
+    if (lane == 20) rec[R_HD] = hole_depths_total(b);
+    if (lane == 21) {
+        rec[R_CLEARS] = 0;
+        rec[R_TOT] = c.holes | (c.maxh << 8) | (uint32_t(c.pw[W]) << 13) | (uint32_t(c.pp[W]) << 17);
+    }
+    __syncwarp();
+}
+
+// search_move_beam (beam.hpp:484-570) for the warp's committed game
+__device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, int lane, uint32_t& evals,
+                                            uint32_t* status) {
+    Move mv{0, 0, 0, true};
+    if (ws.eng.over) return mv;
+    uint32_t slot_piece[NSLOTS];                                  // beam.hpp:226-237
+    slot_piece[0] = ws.eng.held;
+    slot_piece[1] = ws.eng.queue[0];
+#pragma unroll
+    for (int i = 0; i < DEPTH; ++i) slot_piece[2 + i] = ws.eng.queue[1 + i];
+    int const tree = ws.eng.held == NO_PIECE ? 1 : 0;
+    uint32_t const r0 = c_tables.node[tree][0][0], r1 = c_tables.node[tree][0][1];
+    uint32_t const p0 = slot_piece[r0 & 0xFu], p1 = slot_piece[r1 & 0xFu];
+
+    int kept = 1;                              // frontier size feeding the next stage
+    uint32_t fscore = 0, fnode = 0, frank = uint32_t(lane), root_slot = 0;
+    uint64_t best = 0;                         // leaf-order (score | order) maximum, fallbacks included
+#pragma unroll 1
+    for (int stage = 0; stage < DEPTH; ++stage) {
+        bool const leaf = stage == DEPTH - 1;
+        // ---- segments of this stage
+        uint32_t total;
+        if (stage == 0) {                      // two root groups over the committed board (beam.hpp:283-301)
+            root_record(&ws, lane);
+            if (lane < 2) {
+                uint32_t const nd = lane ? r1 : r0;
+                uint32_t const held_slot = (nd >> 4) & 0xFu;
+                uint32_t const held_i = held_slot != HELD_NONE && slot_piece[held_slot] == 0u;
+                ws.seg_info[lane] = 32u | ((lane ? p1 : p0) << 16) | (held_i << 20) | (uint32_t(lane) << 21);
+            }
+            total = c_tables.nplace[p0] + c_tables.nplace[p1];
+            if (lane == 0) {
+                ws.seg_off[0] = 0;
+                ws.seg_off[1] = c_tables.nplace[p0];
+                ws.seg_off[2] = total;
+                ws.seg_off[3] = total;
+            }
+            __syncwarp();
+        } else {
+            total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
+        }
+        // ---- every candidate of the stage
+        LevelAcc const a = level_pass(ws, lut, fw, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane, evals);
+        if (stage == 0) {
+            // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
+            kept = __popc(__ballot_sync(FULL_MASK, a.list != 0));
+            if (kept == 0) return mv;                             // no legal root: game over
+            root_slot = 0xFFFFFFFFu - uint32_t(a.list);
+            fscore = uint32_t(a.list >> 32);
+            uint32_t const g = lane < kept ? root_slot / MP : 0u;
+            fnode = g;
+            materialize(&ws, lut, lane < kept, 32u, g ? p1 : p0, root_slot % MP, lane);
+        } else if (!leaf) {
+            uint32_t const has_child = __reduce_or_sync(FULL_MASK, a.lo);
+            // kept nodes with no legal continuation become leaves at this depth (beam.hpp:549-551)
+            if (lane < kept && !((has_child >> lane) & 1u)) {
+                uint64_t const fk = (uint64_t(fscore) << 32) | uint64_t(ORDER_SPAN - (LEAF_ORDERS + frank));
+                best = fk > best ? fk : best;
+            }
+            int const next = __popc(__ballot_sync(FULL_MASK, a.list != 0));
+            // advance the frontier (beam.hpp:379-403): lane j builds kept node j
+            uint32_t const sslot = 0xFFFFFFFFu - uint32_t(a.list);
+            uint32_t const pk = lane < next ? sslot / (2 * MP) : 0u;
+            uint32_t const child = (sslot / MP) & 1u;
+            uint32_t const par_node = __shfl_sync(FULL_MASK, fnode, int(pk));
+            uint32_t const par_rank = __shfl_sync(FULL_MASK, frank, int(pk));
+            uint32_t const cnode = (2u * par_node + child) & 15u;
+            uint32_t const piece = slot_piece[c_tables.node[tree][stage][cnode] & 0xFu];
+            materialize(&ws, lut, lane < next, pk, piece, sslot % MP, lane);
+            fscore = uint32_t(a.list >> 32);
+            fnode = lane < next ? cnode : 0u;
+            frank = par_rank;
+            kept = next;
+        } else {
+            // ---- leaf stage (beam.hpp:407-443): a list whose piece never fit scores the frontier board
+            uint32_t const legal_lo = __reduce_or_sync(FULL_MASK, a.lo);
+            uint32_t const legal_hi = __reduce_or_sync(FULL_MASK, a.hi);
+            best = a.best > best ? a.best : best;
+#pragma unroll
+            for (int half = 0; half < 2; ++half) {
+                int const j = lane + 32 * half;
+                int const k = j >> 1;
+                uint32_t const sc = __shfl_sync(FULL_MASK, fscore, k & 31);
+                bool const legal = ((half ? legal_hi : legal_lo) >> lane) & 1u;
+                if (k < kept && !legal) {
+                    uint64_t const key = (uint64_t(sc) << 32) | uint64_t(ORDER_SPAN - uint32_t(j) * MP);
+                    best = key > best ? key : best;
+                }
+            }
+        }
+    }
+    best = warp_max64(best);
+    if (best == 0) {                                              // unreachable with >= 1 root
+        if (lane == 0) atomicOr(status, 1u);
+        return mv;
+    }
+    // ---- decode the winning key back to its root move (beam.hpp:450-470)
+    uint32_t const order = ORDER_SPAN - uint32_t(best);
+    uint32_t const leaf_rank = __shfl_sync(FULL_MASK, frank, int((order / (2 * MP)) & 31u));
+    uint32_t const rank = order >= uint32_t(LEAF_ORDERS) ? order - LEAF_ORDERS : leaf_rank;
+    uint32_t const rs = __shfl_sync(FULL_MASK, root_slot, int(rank & 31u));
+    uint32_t const g = rs / MP;
+    uint32_t const pa = lut.move[g ? p1 : p0][rs % MP];
+    mv.orient = int((pa >> 20) & 3u);
+    mv.x = int((pa >> 24) & 0xFu) - 2;
+    mv.hold = int((c_tables.node[tree][0][g] >> 8) & 1u);
+    mv.none = ordered_bits_inv(uint32_t(best >> 32)) == -__int_as_float(0x7f800000);   // search.hpp:41
+    return mv;
+}
+
+template <int WARPS, int MINB>
+__global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
+    extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
+    __shared__ LutTables s_lut;
+    for (int t = int(threadIdx.x); t < NPIECE * MP; t += WARPS * 32) {
+        s_lut.fast[t / MP][t % MP] = g_lut.fast[t / MP][t % MP];
+        s_lut.move[t / MP][t % MP] = g_lut.move[t / MP][t % MP];
+    }
+    __syncthreads();
+    Luts const lut{s_lut.fast, s_lut.move};
     int const lane = int(threadIdx.x & 31u);
-    WarpShared& ws = s_warp[threadIdx.x >> 5];
+    WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
     for (;;) {
         uint32_t sim = 0;
         if (lane == 0) sim = atomicAdd(&p.scratch[0], 1u);
-        sim = __shfl_sync(0xFFFFFFFFu, sim, 0);
+        sim = __shfl_sync(FULL_MASK, sim, 0);
         if (sim >= p.total_sims) break;
         uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
-        Model m;
         float const* wsrc = p.weights + size_t(mdl) * NPARAMS;
-#pragma unroll
-        for (int i = 0; i < NPARAMS; ++i) m.w[i] = __ldg(wsrc + i);
+        if (p.timing && lane == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            p.timing[2 * size_t(sim)] = t;
+        }
+        FastW fw;
+        load_fast_weights(GlobalW{wsrc}, fw);
+        for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
         if (lane == 0) {
             engine_reset(ws.eng, seed);
             ws.st = Stats{};
@@ -669,7 +666,7 @@ __global__ void __launch_bounds__(WARPS * 32) eval_kernel(Params p) {
         __syncwarp();
         uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move(ws, m, lane, evals, &p.scratch[1]);
+            Move const mv = search_move(ws, lut, fw, lane, evals, &p.scratch[1]);
             if (mv.none) break;
             if (lane == 0) {
                 if (p.trace) {
@@ -687,7 +684,7 @@ __global__ void __launch_bounds__(WARPS * 32) eval_kernel(Params p) {
             __syncwarp();
             if (ws.eng.over == 2) break;
         }
-        evals = __reduce_add_sync(0xFFFFFFFFu, evals);
+        evals = __reduce_add_sync(FULL_MASK, evals);
         if (lane == 0) {
             p.score[sim] = final_score(ws.st);
             if (p.pieces) p.pieces[sim] = ws.st.pieces;
@@ -696,12 +693,58 @@ __global__ void __launch_bounds__(WARPS * 32) eval_kernel(Params p) {
             if (p.n_moves) p.n_moves[sim] = moves;
             if (p.board_out)
                 for (int x = 0; x < W; ++x) p.board_out[size_t(sim) * W + x] = ws.eng.board[x];
+            if (p.timing) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                p.timing[2 * size_t(sim) + 1] = t;
+            }
         }
         __syncwarp();
     }
 }
 
-constexpr int kWarpsPerBlock = 4;
+// Device self-test of the candidate core (tests only): one thread per
+// candidate, fast path and full path on caller-built records. cand[t] =
+// piece | placement << 8 | held-is-I << 16 | record index << 17.
+__global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand, uint32_t n, float const* w,
+                                     float* fast_v, int* fast_st, float* full_v, int* full_legal, float* dbg) {
+    uint32_t const t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    uint32_t const c = cand[t];
+    uint32_t const piece = c & 0xFFu, i = (c >> 8) & 0xFFu, held = (c >> 16) & 1u;
+    uint32_t const* rec = recs + size_t(c >> 17) * REC_WORDS;
+    FastW fw;
+    load_fast_weights(GlobalW{w}, fw);
+    float v = 0.0f;
+    // the kernel's own arithmetic mode, then (diagnostics only) the packed-PTX mode
+    fast_st[t] = fast_candidate(rec, g_lut.fast[piece][i], held, fw, v, dbg ? dbg + size_t(t) * 32 : nullptr);
+    if (dbg) {
+        float v2 = 0.0f;
+        fast_candidate<MLP_PTX_X2>(rec, g_lut.fast[piece][i], held, fw, v2, nullptr);
+        dbg[size_t(t) * 32 + 31] = v2;
+    }
+    fast_v[t] = v;
+    uint32_t const mv = g_lut.move[piece][i];
+    uint32_t b[W], nb[W];
+    for (int x = 0; x < W; ++x) b[x] = rec[R_BOARD + x];
+    int cl = 0;
+    full_legal[t] = apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl);
+    full_v[t] = full_legal[t] ? value_full(rec[R_CLEARS] + clear_bump(cl), board_ints(nb), held, GlobalW{w}) : 0.0f;
+}
+
+// Launch-shape variants (warps per block, minimum resident blocks per SM =
+// the register cap): the autotuner's search space.
+using KernelFn = void (*)(Params);
+struct Variant {
+    KernelFn fn;
+    uint32_t warps, min_blocks;
+};
+Variant const kVariants[] = {
+    {eval_kernel<4, 3>, 4, 3}, {eval_kernel<4, 4>, 4, 4}, {eval_kernel<4, 5>, 4, 5}, {eval_kernel<4, 6>, 4, 6},
+    {eval_kernel<2, 10>, 2, 10}, {eval_kernel<2, 12>, 2, 12},
+};
+constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
+constexpr int kDefaultVariant = 2;
 
 } // namespace
 } // namespace ta3b
@@ -712,7 +755,8 @@ using namespace ta3b;
 struct ta3b_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    uint32_t warps_per_block = kWarpsPerBlock;
+    int variant = kDefaultVariant;
+    uint32_t warps_per_block = 0;
     uint32_t blocks_per_sm = 0;
     uint32_t sms = 0;
     uint32_t grid = 0;
@@ -731,6 +775,8 @@ struct ta3b_ctx {
     uint32_t* d_board = nullptr;
     size_t cap_tb = 0;
     uint32_t* d_scratch = nullptr;
+    uint64_t* d_timing = nullptr;
+    size_t cap_timing = 0;
     std::string err;
 };
 
@@ -780,7 +826,7 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st) {
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, 2 * sizeof(uint32_t), st), "reset work queue");
     uint32_t const need_blocks = (prm.total_sims + ctx->warps_per_block - 1) / ctx->warps_per_block;
     uint32_t const grid = need_blocks < ctx->grid ? need_blocks : ctx->grid;
-    eval_kernel<kWarpsPerBlock><<<grid, ctx->warps_per_block * 32, 0, st>>>(prm);
+    kVariants[ctx->variant].fn<<<grid, ctx->warps_per_block * 32, ctx->warps_per_block * sizeof(WarpShared), st>>>(prm);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     return TA3B_OK;
 }
@@ -797,7 +843,7 @@ int read_status(ta3b_ctx* ctx) {
 int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_t mpi, uint32_t num_params,
               uint64_t const* seeds, uint32_t num_games, uint32_t max_moves, float* score_out, uint32_t* pieces_out,
               uint32_t* lines_out, uint32_t* evals_out, uint8_t* trace_out, uint32_t* nmoves_out,
-              uint32_t* board_out) {
+              uint32_t* board_out, uint64_t* timing_out = nullptr) {
     if (int rc = check_sizes(ctx, num_islands, mpi, num_params, num_games)) return rc;
     uint64_t const models = uint64_t(num_islands) * mpi;
     uint64_t const sims = models * num_games;
@@ -818,6 +864,8 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
         ctx->cap_sims = sims;
     }
     bool const tracing = trace_out || nmoves_out || board_out;
+    if (timing_out)
+        if (int rc = grow(ctx, ctx->d_timing, ctx->cap_timing, 2 * sims, "alloc timing")) return rc;
     if (tracing) {
         if (int rc = grow(ctx, ctx->d_trace, ctx->cap_trace, sims * max_moves * 3 + 1, "alloc trace")) return rc;
         if (ctx->cap_tb < sims) {
@@ -843,6 +891,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     prm.n_moves = tracing ? ctx->d_nmoves : nullptr;
     prm.board_out = tracing ? ctx->d_board : nullptr;
     prm.scratch = ctx->d_scratch;
+    prm.timing = timing_out ? reinterpret_cast<unsigned long long*>(ctx->d_timing) : nullptr;
     prm.num_games = num_games;
     prm.models_per_island = mpi;
     prm.max_moves = max_moves;
@@ -868,7 +917,29 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     if (board_out)
         TA3B_CUDA(ctx, cudaMemcpyAsync(board_out, ctx->d_board, sims * W * 4, cudaMemcpyDeviceToHost, ctx->stream),
                   "copy boards");
+    if (timing_out)
+        TA3B_CUDA(ctx, cudaMemcpyAsync(timing_out, ctx->d_timing, sims * 16, cudaMemcpyDeviceToHost, ctx->stream),
+                  "copy timing");
     return read_status(ctx);
+}
+
+int select_variant(ta3b_ctx* ctx, int v) {
+    if (v < 0 || v >= kNumVariants) return fail(ctx, TA3B_ERR_ARG, "variant out of range");
+    TA3B_CUDA(ctx, cudaSetDevice(ctx->device), "set device");
+    size_t const dyn = kVariants[v].warps * sizeof(WarpShared);
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(kVariants[v].fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)),
+              "dynamic smem size");
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(kVariants[v].fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared), "smem carveout");
+    int per_sm = 0;
+    TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].fn, kVariants[v].warps * 32, dyn),
+              "occupancy");
+    if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "kernel variant does not fit on an SM");
+    ctx->variant = v;
+    ctx->warps_per_block = kVariants[v].warps;
+    ctx->blocks_per_sm = uint32_t(per_sm);
+    ctx->grid = ctx->sms * ctx->blocks_per_sm;
+    return TA3B_OK;
 }
 
 } // namespace
@@ -900,11 +971,6 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
     auto* ctx = new ta3b_ctx();
     ctx->device = c.device;
     ctx->sms = uint32_t(prop.multiProcessorCount);
-    if (c.warps_per_block && c.warps_per_block != kWarpsPerBlock) {
-        g_create_error = "warps_per_block must be 0 or " + std::to_string(kWarpsPerBlock);
-        delete ctx;
-        return nullptr;
-    }
     if (cudaSetDevice(c.device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_scratch, 4 * sizeof(uint32_t)) != cudaSuccess) {
@@ -912,12 +978,26 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
         ta3b_destroy(ctx);
         return nullptr;
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eval_kernel<kWarpsPerBlock>, kWarpsPerBlock * 32, 0);
-    if (per_sm < 1) per_sm = 1;
-    ctx->blocks_per_sm = c.blocks_per_sm ? (c.blocks_per_sm < uint32_t(per_sm) ? c.blocks_per_sm : uint32_t(per_sm))
-                                         : uint32_t(per_sm);
-    ctx->grid = ctx->sms * ctx->blocks_per_sm;
+    int v = kDefaultVariant;
+    if (c.warps_per_block || c.blocks_per_sm) {
+        v = -1;
+        for (int i = 0; i < kNumVariants; ++i)
+            if ((!c.warps_per_block || kVariants[i].warps == c.warps_per_block) &&
+                (!c.blocks_per_sm || kVariants[i].min_blocks == c.blocks_per_sm)) {
+                v = i;
+                break;
+            }
+        if (v < 0) {
+            g_create_error = "no kernel variant with that warps_per_block / blocks_per_sm (see ta3b_variant_info)";
+            ta3b_destroy(ctx);
+            return nullptr;
+        }
+    }
+    if (select_variant(ctx, v) != TA3B_OK) {
+        g_create_error = ctx->err;
+        ta3b_destroy(ctx);
+        return nullptr;
+    }
     return ctx;
 }
 
@@ -925,7 +1005,7 @@ void ta3b_destroy(ta3b_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     void* bufs[] = {ctx->d_w, ctx->d_seeds, ctx->d_score, ctx->d_pieces, ctx->d_lines, ctx->d_evals,
-                    ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch};
+                    ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -953,6 +1033,13 @@ int ta3b_eval_trace(ta3b_ctx* ctx, float const* weights, uint32_t num_models, ui
                     uint32_t* n_moves_out, uint32_t* board_out) {
     return host_eval(ctx, weights, 1, num_models, num_params, seeds, num_games, max_moves, score_out, pieces_out,
                      lines_out, evals_out, trace_out, n_moves_out, board_out);
+}
+
+int ta3b_eval_timed(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_t models_per_island,
+                    uint32_t num_params, uint64_t const* seeds, uint32_t num_games, uint32_t max_moves,
+                    float* score_out, uint32_t* pieces_out, uint32_t* evals_out, uint64_t* timing_out) {
+    return host_eval(ctx, weights, num_islands, models_per_island, num_params, seeds, num_games, max_moves, score_out,
+                     pieces_out, nullptr, evals_out, nullptr, nullptr, nullptr, timing_out);
 }
 
 int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands, uint32_t models_per_island,
@@ -999,6 +1086,54 @@ int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out) {
         seeds_out[g] = r;
     }
     return TA3B_OK;
+}
+
+int ta3b_core_selftest(uint32_t const* recs, uint32_t num_recs, uint32_t const* cand, uint32_t n, float const* w97,
+                       float* fast_v, int* fast_st, float* full_v, int* full_legal, float* dbg32) {
+    if (!recs || !cand || !w97 || !fast_v || !fast_st || !full_v || !full_legal) return TA3B_ERR_ARG;
+    if (n == 0) return TA3B_OK;
+    void* d[8] = {};
+    size_t const sz[8] = {size_t(num_recs) * REC_WORDS * 4, size_t(n) * 4, NPARAMS * 4, size_t(n) * 4, size_t(n) * 4,
+                          size_t(n) * 4, size_t(n) * 4, dbg32 ? size_t(n) * 32 * 4 : 4};
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaMalloc(&d[k], sz[k]);
+    if (e == cudaSuccess) e = cudaMemcpy(d[0], recs, sz[0], cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d[1], cand, sz[1], cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d[2], w97, sz[2], cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        core_selftest_kernel<<<(n + 127) / 128, 128>>>(static_cast<uint32_t*>(d[0]), static_cast<uint32_t*>(d[1]), n,
+                                                        static_cast<float*>(d[2]), static_cast<float*>(d[3]),
+                                                        static_cast<int*>(d[4]), static_cast<float*>(d[5]),
+                                                        static_cast<int*>(d[6]),
+                                                        dbg32 ? static_cast<float*>(d[7]) : nullptr);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(fast_v, d[3], sz[3], cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(fast_st, d[4], sz[4], cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(full_v, d[5], sz[5], cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(full_legal, d[6], sz[6], cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && dbg32) e = cudaMemcpy(dbg32, d[7], sz[7], cudaMemcpyDeviceToHost);
+    for (void* q : d)
+        if (q) cudaFree(q);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("core selftest: ") + cudaGetErrorString(e);
+        return TA3B_ERR_CUDA;
+    }
+    return TA3B_OK;
+}
+
+int ta3b_num_variants(void) { return kNumVariants; }
+
+int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm) {
+    if (variant < 0 || variant >= kNumVariants) return TA3B_ERR_ARG;
+    if (warps_per_block) *warps_per_block = kVariants[variant].warps;
+    if (min_blocks_per_sm) *min_blocks_per_sm = kVariants[variant].min_blocks;
+    return TA3B_OK;
+}
+
+int ta3b_select_variant(ta3b_ctx* ctx, int variant) {
+    if (!ctx) return TA3B_ERR_ARG;
+    return select_variant(ctx, variant);
 }
 
 int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms) {

@@ -174,6 +174,113 @@ constexpr Tables make_tables() {
 
 constexpr Tables TABLES = make_tables();
 
+// Per-placement data for the incremental candidate path (16 bytes):
+//   d4  byte i = 22 - lowest cell row of piece column i (i < width), 127 beyond
+//   c4  byte i = cells in piece column i (i < width), 0 beyond
+//   m   cells per local row r (nibble r, 16 bits) | combo id (6) << 16 | width==1 << 22
+//       | has left neighbour column << 23 | has right neighbour column << 24
+//       | min over columns of the highest cell row (2) << 25 | window origin c0 (4) << 27
+//   s   sum_{i<w} (22 - low_i) (7) | sum_i cells_i * (22 - low_i) (7) << 7
+//       | sum of squared top-row steps inside the piece (4) << 14 | top row of column 0 (2) << 18
+//       | top row of the last column (2) << 20 | width (3) << 22
+// A combo is one (window origin c0, width w) pair; the 34 combos index the
+// per-parent table of old surface / well terms.
+struct PlaceFast {
+    uint32_t d4, c4, m, s;
+};
+
+constexpr int combo_id(int c0, int w) {
+    return (w == 1 ? 0 : w == 2 ? 10 : w == 3 ? 19 : 27) + c0;
+}
+constexpr int NCOMBO = 34;
+
+constexpr PlaceFast make_place_fast(Place p) {
+    uint32_t width = 0, pr = 0;
+    uint32_t low[4]{}, first[4]{}, cnt[4]{};
+    for (int i = 0; i < 4; ++i) {
+        uint32_t const nib = (uint32_t(p.cols) >> (4 * i)) & 0xFu;
+        if (!nib) continue;
+        width = uint32_t(i + 1);
+        uint32_t lo = 0, fi = 3, n = 0;
+        for (uint32_t r = 0; r < 4; ++r)
+            if ((nib >> r) & 1u) {
+                lo = r;
+                if (r < fi) fi = r;
+                ++n;
+                pr += 1u << (4 * r);
+            }
+        low[i] = lo;
+        first[i] = fi;
+        cnt[i] = n;
+    }
+    uint32_t d4 = 0, c4 = 0, a1 = 0, a2 = 0, sint = 0, minfirst = 3;
+    for (uint32_t i = 0; i < 4; ++i) {
+        uint32_t const d = i < width ? 22u - low[i] : 127u;
+        d4 |= d << (8 * i);
+        c4 |= (i < width ? cnt[i] : 0u) << (8 * i);
+        if (i < width) {
+            a1 += 22u - low[i];
+            a2 += cnt[i] * (22u - low[i]);
+            if (first[i] < minfirst) minfirst = first[i];
+            if (i + 1 < width) {
+                int const step = int(first[i]) - int(first[i + 1]);
+                sint += uint32_t(step * step);
+            }
+        }
+    }
+    int const c0 = p.col0;
+    uint32_t const m = pr | (uint32_t(combo_id(c0, int(width))) << 16) | (uint32_t(width == 1) << 22) |
+                       (uint32_t(c0 > 0) << 23) | (uint32_t(c0 + int(width) < W) << 24) | (minfirst << 25) |
+                       (uint32_t(c0) << 27);
+    uint32_t const s = a1 | (a2 << 7) | (sint << 14) | (first[0] << 18) | (first[width - 1] << 20) | (width << 22);
+    return PlaceFast{d4, c4, m, s};
+}
+
+struct FastTables {
+    PlaceFast place[NPIECE][MP];
+};
+
+constexpr FastTables make_fast_tables() {
+    FastTables f{};
+    for (int p = 0; p < NPIECE; ++p)
+        for (int i = 0; i < TABLES.nplace[p]; ++i) f.place[p][i] = make_place_fast(TABLES.place[p][i]);
+    return f;
+}
+
+constexpr FastTables FAST = make_fast_tables();
+
+// adjacent piece columns' top rows differ by at most 2, so no column inside a
+// piece's span can be a well (depth >= 3) right after the drop
+constexpr bool span_has_no_wells() {
+    for (int p = 0; p < NPIECE; ++p)
+        for (int i = 0; i < TABLES.nplace[p]; ++i) {
+            PlaceFast const f = FAST.place[p][i];
+            uint32_t const w = (f.s >> 22) & 7u;
+            for (uint32_t c = 0; c + 1 < w; ++c) {
+                uint32_t const nib0 = (uint32_t(TABLES.place[p][i].cols) >> (4 * c)) & 0xFu;
+                uint32_t const nib1 = (uint32_t(TABLES.place[p][i].cols) >> (4 * (c + 1))) & 0xFu;
+                int f0 = 0, f1 = 0;
+                while (!((nib0 >> f0) & 1u)) ++f0;
+                while (!((nib1 >> f1) & 1u)) ++f1;
+                if (f0 - f1 > 2 || f1 - f0 > 2) return false;
+            }
+        }
+    return true;
+}
+static_assert(span_has_no_wells(), "piece columns' top rows must differ by <= 2");
+
+// every tetromino column is one contiguous run of cells (the incremental path relies on it)
+constexpr bool columns_contiguous() {
+    for (int p = 0; p < NPIECE; ++p)
+        for (int o = 0; o < 4; ++o)
+            for (int i = 0; i < 4; ++i) {
+                uint32_t const nib = (uint32_t(TABLES.shape_cols[p][o]) >> (4 * i)) & 0xFu;
+                if (nib && ((nib + (nib & (~nib + 1u))) & nib)) return false;
+            }
+    return true;
+}
+static_assert(columns_contiguous(), "piece columns must be contiguous");
+
 // Known answers from the reference tests (ta3_ai/tests/src/search/search_test.cpp:60-67).
 static_assert(TABLES.nplace[0] == 17 && TABLES.nplace[1] == 9 && TABLES.nplace[2] == 34 && TABLES.nplace[3] == 17 &&
               TABLES.nplace[4] == 17 && TABLES.nplace[5] == 34 && TABLES.nplace[6] == 34, "placement counts");

@@ -21,7 +21,8 @@ _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "li
 _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
-           "ta3b_eval_trace", "ta3b_simulate_seeds", "ta3b_launch_info"]
+           "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
+           "ta3b_select_variant", "ta3b_core_selftest"]
 
 
 class EvaluatorError(RuntimeError):
@@ -51,8 +52,13 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_eval_islands.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp]
     lib.ta3b_eval_device.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp]
     lib.ta3b_eval_trace.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp]
+    lib.ta3b_eval_timed.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp]
     lib.ta3b_simulate_seeds.argtypes = [u64, u32, vp]
     lib.ta3b_launch_info.argtypes = [vp, vp, vp, vp]
+    lib.ta3b_num_variants.argtypes = []
+    lib.ta3b_variant_info.argtypes = [C.c_int, vp, vp]
+    lib.ta3b_select_variant.argtypes = [vp, C.c_int]
+    lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
     if path is None:
         _lib = lib
     return lib
@@ -134,6 +140,18 @@ class ModelEvaluator:
                                                 _p(sc), _p(pc), _p(lc)))
         return sc, pc, lc
 
+    def eval_timed(self, weights, seeds_per_island, max_moves: int):
+        """Island batch plus per-sim scheduling data: (score, pieces, evals, timing[n, 2] ns)."""
+        s = np.ascontiguousarray(seeds_per_island, dtype=np.uint64)
+        islands, games = s.shape
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1, NUM_PARAMS)
+        n = w.shape[0] * games
+        sc, pc, ec = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        tm = np.zeros((n, 2), np.uint64)
+        self._check(self._lib.ta3b_eval_timed(self._ctx, _p(w), islands, w.shape[0] // islands, NUM_PARAMS, _p(s),
+                                              games, max_moves, _p(sc), _p(pc), _p(ec), _p(tm)))
+        return sc, pc, ec, tm
+
     def eval_trace(self, weights, num_models: int, seeds, max_moves: int):
         """Everything, plus per-move traces: dict of model-major arrays."""
         w, s = self._prep(weights, num_models, seeds)
@@ -159,6 +177,40 @@ class ModelEvaluator:
         self._check(self._lib.ta3b_eval_device(self._ctx, ptr(weights), islands, models // islands, NUM_PARAMS,
                                                ptr(seeds), games, max_moves, ptr(score), ptr(pieces), ptr(lines),
                                                ptr(evals), st))
+
+    def select_variant(self, variant: int):
+        self._check(self._lib.ta3b_select_variant(self._ctx, variant))
+
+    @staticmethod
+    def variants():
+        lib = library()
+        out = []
+        for v in range(lib.ta3b_num_variants()):
+            w, b = C.c_uint32(), C.c_uint32()
+            lib.ta3b_variant_info(v, C.byref(w), C.byref(b))
+            out.append({"variant": v, "warps_per_block": w.value, "min_blocks_per_sm": b.value})
+        return out
+
+    def autotune(self, weights, seeds, max_moves: int, score, pieces=None, lines=None, evals=None,
+                 num_islands: int = 1, stream=None, reps: int = 1):
+        """Time every launch-shape variant on this device batch (CUDA events on
+        `stream`) and keep the fastest. Returns {variant: ms}."""
+        import torch
+        times = {}
+        st = stream or torch.cuda.current_stream()
+        for v in range(len(self.variants())):
+            self.select_variant(v)
+            with torch.cuda.stream(st):
+                self.eval_device(weights, seeds, max_moves, score, pieces, lines, evals, num_islands, st)  # warm
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                for _ in range(reps):
+                    self.eval_device(weights, seeds, max_moves, score, pieces, lines, evals, num_islands, st)
+                b.record(st)
+            b.synchronize()
+            times[v] = a.elapsed_time(b) / reps
+        self.select_variant(min(times, key=times.get))
+        return times
 
     def launch_info(self):
         g, w, s = C.c_uint32(), C.c_uint32(), C.c_uint32()
