@@ -129,6 +129,8 @@ struct Cand {
     bool legal;
 };
 
+unsigned long long g_fast_count = 0, g_defer_count = 0;
+
 // one candidate through the kernel's paths
 Cand candidate(uint32_t const* rec, int piece, int i, bool held, bool leaf, uint32_t k, uint32_t child,
                FastW const& fw, HostW const& w) {
@@ -140,7 +142,9 @@ Cand candidate(uint32_t const* rec, int piece, int i, bool held, bool leaf, uint
     r.h4 = rec[R_SPAN + 2 * c0]; r.hm4 = rec[R_SPAN + 2 * c0 + 1];
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
     float v;
-    if (fast_eval<MLP_SCALAR>(r, pf, held, fw, v) != FAST_OK) {
+    bool const fast = fast_eval<MLP_SCALAR>(r, pf, held, fw, v) == FAST_OK;
+    ++(fast ? g_fast_count : g_defer_count);
+    if (!fast) {
         uint32_t b[W], nb[W];
         for (int x = 0; x < W; ++x) b[x] = rec[R_BOARD + x];
         Place const pl = TABLES.place[piece][i];
@@ -162,8 +166,30 @@ void child_record(uint32_t const* prec, int piece, int i, HostW const& w, uint32
     build_record(nb, prec[R_CLEARS] + clear_bump(cl), w, out);
 }
 
+unsigned long long g_insertions = 0, g_rounds = 0, g_levels = 0, g_cands = 0;
+
+// insertions the warp's top-k fold performs when the keys arrive 32 per round in
+// flattened order (a key is inserted when it beats the current k-th best)
+void count_insertions(std::vector<uint64_t> const& keys, size_t k) {
+    std::vector<uint64_t> list;
+    ++g_levels;
+    for (size_t r = 0; r < keys.size(); r += 32) {
+        ++g_rounds;
+        for (size_t l = r; l < keys.size() && l < r + 32; ++l) {
+            uint64_t const thr = list.size() < k ? 0 : list[k - 1];
+            if (keys[l] > thr) {
+                ++g_insertions;
+                list.insert(std::upper_bound(list.begin(), list.end(), keys[l], [](uint64_t a, uint64_t b) { return a > b; }), keys[l]);
+                if (list.size() > k) list.pop_back();
+            }
+        }
+    }
+    g_cands += keys.size();
+}
+
 // top-k of (key) with keys unique; returns sorted descending
 std::vector<uint64_t> topk(std::vector<uint64_t> keys, size_t k) {
+    count_insertions(keys, k);
     std::sort(keys.begin(), keys.end(), [](uint64_t a, uint64_t b) { return a > b; });
     while (!keys.empty() && keys.back() == 0) keys.pop_back();
     if (keys.size() > k) keys.resize(k);
@@ -173,6 +199,19 @@ std::vector<uint64_t> topk(std::vector<uint64_t> keys, size_t k) {
 } // namespace
 
 extern "C" {
+
+void ta3bt_path_counts(unsigned long long* fast, unsigned long long* deferred) {
+    *fast = g_fast_count;
+    *deferred = g_defer_count;
+}
+
+void ta3bt_topk_counts(unsigned long long* ins, unsigned long long* rounds, unsigned long long* levels,
+                       unsigned long long* cands) {
+    *ins = g_insertions;
+    *rounds = g_rounds;
+    *levels = g_levels;
+    *cands = g_cands;
+}
 
 // root record the way the warp builds it (each "lane" writes its own words)
 void ta3bt_root_record(uint32_t const* b10, float const* w97, uint32_t* rec) {

@@ -299,8 +299,9 @@ TA3B_HD int dot4_s8(uint32_t a, uint32_t b) {                   // sum of 4 sign
 }
 
 // ------------------------------------------------------ parent record ---
-// One kept frontier node (or the committed board), in 80 u32 words:
-constexpr int REC_WORDS = 80;
+// One kept frontier node (or the committed board), in 84 u32 words (80 used;
+// the padding staggers the records across shared-memory banks):
+constexpr int REC_WORDS = 84;
 constexpr int R_P = 0;        // float[8]: hidden partial sums after the 4 clear inputs
 constexpr int R_BOARD = 8;    // 10 bit-columns
 constexpr int R_CLEARS = 18;  // path clear histogram (4 x 8-bit lanes)
@@ -378,6 +379,7 @@ TA3B_HD uint32_t row_counts(uint32_t const (&b)[W], int q) {
 
 TA3B_HD void span_words(ColumnData const& c, int c0, uint32_t& h4, uint32_t& hm4) {
     h4 = hm4 = 0;
+#pragma unroll
     for (int i = 0; i < 4; ++i) {
         int const x = c0 + i;
         if (x < W) {
@@ -434,9 +436,10 @@ TA3B_HD void build_record(uint32_t const (&b)[W], uint32_t clear_bits, WF const&
     rec[R_HD] = hole_depths_total(b);
 #pragma unroll
     for (int q = 0; q < 3; ++q) rec[R_RC + q] = row_counts(b, q);
-#pragma unroll 1
+    // fully unrolled: every column index is a constant, so the column data stays in registers
+#pragma unroll
     for (int c0 = 0; c0 < W; ++c0) span_words(c, c0, rec[R_SPAN + 2 * c0], rec[R_SPAN + 2 * c0 + 1]);
-#pragma unroll 1
+#pragma unroll
     for (int id = 0; id < NCOMBO; ++id) {
         int c0, wd;
         combo_of(id, c0, wd);

@@ -214,6 +214,9 @@ __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uin
     b[8] = q2.x; b[9] = q2.y;
 }
 
+#ifndef TA3B_ILP
+#define TA3B_ILP 1
+#endif
 #ifndef TA3B_MLP_MODE
 #define TA3B_MLP_MODE MLP_SCALAR
 #endif
@@ -274,12 +277,13 @@ __device__ __forceinline__ uint64_t shfl64_up(uint64_t v) {
 }
 
 // Fold one key per lane into the warp's sorted top-K list (lane i = i-th
-// largest, 0 = empty). Keys are unique per level (the low word encodes the
-// slot), so the kept set equals beam.hpp:244-265's "max score, lowest slot on
-// ties" whatever the insertion order.
-__device__ __forceinline__ void topk_fold(uint64_t& list, uint64_t key, int k, int lane) {
-    uint64_t thr = shfl64(list, k - 1);
+// largest, 0 = empty; `thr` caches list[k-1]). Keys are unique per level (the
+// low word encodes the slot), so the kept set equals beam.hpp:244-265's "max
+// score, lowest slot on ties" whatever the order keys arrive in. (A bitonic
+// sort-and-merge of whole rounds measured slower than these insertions.)
+__device__ __forceinline__ void topk_fold(uint64_t& list, uint64_t& thr, uint64_t key, int k, int lane) {
     uint32_t mask = __ballot_sync(FULL_MASK, key > thr);
+    if (!mask) return;
     while (mask) {
         int const s = __ffs(int(mask)) - 1;
         uint64_t const x = shfl64(key, s);
@@ -335,6 +339,7 @@ struct Move {
 };
 
 struct LevelAcc {
+    uint64_t thr;                      // list[k-1], the key a candidate must beat
     uint64_t list;                     // top-K list (STAGE_TOPK)
     uint64_t best;                     // argmax of leaf keys and fallbacks (STAGE_LEAF)
     uint32_t lo, hi;                   // TOPK: bit k = parent k has a legal child; LEAF: bit = list legal
@@ -374,7 +379,7 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
 // per-parent legality.
 __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, bool leaf, uint32_t total,
                                                int kl, int lane, uint32_t& evals) {
-    LevelAcc acc{0, 0, 0, 0};
+    LevelAcc acc{0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
             ++evals;
@@ -385,7 +390,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
     };
     auto fold = [&](uint64_t key) {
         if (leaf) acc.best = key > acc.best ? key : acc.best;
-        else topk_fold(acc.list, key, kl, lane);
+        else topk_fold(acc.list, acc.thr, key, kl, lane);
     };
     auto drain = [&](uint32_t n, uint32_t queued) {
         uint64_t key = 0;
@@ -405,33 +410,46 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
     };
     uint32_t queued = 0;
     int seg = 0;
-    for (uint32_t c0 = 0; c0 < total; c0 += WARP) {
-        uint32_t const c = c0 + uint32_t(lane);
-        uint64_t key = 0;
-        bool def = false;
-        uint32_t entry = 0;
-        if (c < total) {
-            while (ws.seg_off[seg + 1] <= c) ++seg;
-            uint32_t const info = ws.seg_info[seg];
-            uint32_t const i = c - ws.seg_off[seg];
-            PlaceFast const pf = lut.fast[(info >> 16) & 7u][i];
-            float v;
-            if (fast_candidate(ws.rec[info & 63u], pf, (info >> 20) & 1u, fw, v) == FAST_OK) {
-                key = candidate_key(leaf, v, info, i);
-                consume(key, uint32_t(seg), info);
-            } else {
-                def = true;
-                entry = (uint32_t(seg) << 8) | i;
-            }
+    // TA3B_ILP candidates per lane per iteration (c, c+32, ...) in straight-line
+    // code (1 measured fastest on B200: 504 ms per configs[1] step vs 694 ms for 2)
+    // code, so their dependency chains interleave; out-of-range slots evaluate
+    // the last real candidate and are discarded
+    for (uint32_t c0 = 0; c0 < total; c0 += TA3B_ILP * WARP) {
+        uint32_t info[TA3B_ILP], idx[TA3B_ILP], sg[TA3B_ILP];
+        bool valid[TA3B_ILP];
+#pragma unroll
+        for (int u = 0; u < TA3B_ILP; ++u) {
+            uint32_t const c = c0 + uint32_t(u * WARP + lane);
+            valid[u] = c < total;
+            uint32_t const cc = valid[u] ? c : total - 1u;
+            while (ws.seg_off[seg + 1] <= cc) ++seg;
+            sg[u] = uint32_t(seg);
+            info[u] = ws.seg_info[seg];
+            idx[u] = cc - ws.seg_off[seg];
         }
-        uint32_t const dm = __ballot_sync(FULL_MASK, def);
-        if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = entry;
-        queued += __popc(dm);
-        fold(key);
-        if (queued >= uint32_t(WARP)) {
-            __syncwarp();
-            drain(WARP, queued);
-            queued -= WARP;
+        float v[TA3B_ILP];
+        int st[TA3B_ILP];
+#pragma unroll
+        for (int u = 0; u < TA3B_ILP; ++u)
+            st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]], (info[u] >> 20) & 1u,
+                                   fw, v[u]);
+#pragma unroll
+        for (int u = 0; u < TA3B_ILP; ++u) {
+            uint64_t key = 0;
+            bool const def = valid[u] && st[u] != FAST_OK;
+            if (valid[u] && st[u] == FAST_OK) {
+                key = candidate_key(leaf, v[u], info[u], idx[u]);
+                consume(key, sg[u], info[u]);
+            }
+            uint32_t const dm = __ballot_sync(FULL_MASK, def);
+            if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = (sg[u] << 8) | idx[u];
+            queued += __popc(dm);
+            fold(key);
+            if (queued >= uint32_t(WARP)) {
+                __syncwarp();
+                drain(WARP, queued);
+                queued -= WARP;
+            }
         }
     }
     __syncwarp();
@@ -494,28 +512,12 @@ __device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, 
     __syncwarp();
 }
 
-// the committed board's record (record 32), built by the whole warp
+// the committed board's record (record 32): one lane builds it, the warp waits
 __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
-    uint32_t b[W];
-    load_board(ws->eng.board, b);
-    ColumnData c;
-    column_data(b, c);
-    uint32_t* rec = ws->rec[32];
-    if (lane < W) {
-        rec[R_BOARD + lane] = b[lane];
-        span_words(c, lane, rec[R_SPAN + 2 * lane], rec[R_SPAN + 2 * lane + 1]);
-    }
-    for (int id = lane; id < NCOMBO; id += WARP) {
-        int c0, wd;
-        combo_of(id, c0, wd);
-        rec[R_COMBO + id] = combo_word(c, c0, wd);
-    }
-    if (lane < NHID) rec[R_P + lane] = partial_word(0u, lane, SmemW{ws->wfull});
-    if (lane >= 16 && lane < 19) rec[R_RC + lane - 16] = row_counts(b, lane - 16);
-    if (lane == 20) rec[R_HD] = hole_depths_total(b);
-    if (lane == 21) {
-        rec[R_CLEARS] = 0;
-        rec[R_TOT] = c.holes | (c.maxh << 8) | (uint32_t(c.pw[W]) << 13) | (uint32_t(c.pp[W]) << 17);
+    if (lane == 0) {
+        uint32_t b[W];
+        load_board(ws->eng.board, b);
+        build_record(b, 0u, SmemW{ws->wfull}, ws->rec[32]);
     }
     __syncwarp();
 }

@@ -18,6 +18,7 @@ import numpy as np
 from .workload import NUM_PARAMS
 
 _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libta3b.so")
+# TA3B_LIBRARY may name another build of the same C ABI (e.g. an experimental one)
 _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
@@ -38,7 +39,7 @@ def library(path: str | None = None) -> C.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or _LIB_PATH
+    p = path or os.environ.get("TA3B_LIBRARY") or _LIB_PATH
     if not os.path.exists(p):
         raise EvaluatorError(f"CUDA evaluator library missing: {p} (run python -m tetris_ai3_b200.build)")
     lib = C.CDLL(p)
