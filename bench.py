@@ -38,10 +38,18 @@ from tetris_ai3_b200 import workload  # noqa: E402
 
 METRIC = "beam placements/s on 1 B200 (configs[1]: one CMA-ES generation, 10k sims, cap 2000)"
 UNIT = "placements/s"
-# Lane-instructions the kernel executes per evaluated placement (ncu
-# smsp__thread_inst_executed.sum / placements of the same launch), used for the
-# issue roofline; see profiles/ for the capture it comes from.
-LANE_INSTR_PER_PLACEMENT = float(os.environ.get("TA3B_LANE_INSTR_PER_PLACEMENT", "0") or 0)
+# Issue roofline (the path is INT32/FP32 issue-bound, not HBM- or tensor-bound):
+# REF_OPS_PER_PLACEMENT is the reference algorithm's operation count for one
+# evaluated placement, counted on the restatement: drop/collision over 10 columns
+# (230) + lock (80) + full-row test (12) + clear histogram (3); v11 features
+# (16 + 46 per column x 10 + 11); MLP 8 x (10 mul + 10 add + relu) + 8 mul + 8 add
+# (192); key (6) = 1010.
+REF_OPS_PER_PLACEMENT = 1010
+# What this kernel executes per placement (ncu thread_inst_executed / placements,
+# profiles/eval_kernel_small_case_full.md) and its DRAM bytes per configs[1] launch
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/eval_kernel_configs1_launches.md).
+LANE_INSTR_PER_PLACEMENT = 564
+DRAM_BYTES_PER_LAUNCH = None
 
 
 def _dist_env():
@@ -289,14 +297,15 @@ def run_ours(args):
         sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
         peak_issue = sms * 4 * 32 * sm_mhz * 1e6 / 1e12            # lane-instructions, T/s
         per_gpu = value / world
-        roof = None
-        if LANE_INSTR_PER_PLACEMENT > 0:
-            ach = per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12
-            roof = {"bound": "issue", "achieved": ach, "peak": peak_issue, "unit": "T lane-instr/s",
-                    "frac": ach / peak_issue, "traffic": None,
-                    "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz from MEASURED_PEAKS.json "
-                                   f"({kind})",
-                    "lane_instr_per_placement": LANE_INSTR_PER_PLACEMENT}
+        ach = per_gpu * REF_OPS_PER_PLACEMENT / 1e12
+        roof = {"bound": "issue", "achieved": ach, "peak": peak_issue, "unit": "T int32/fp32 lane-ops/s",
+                "frac": ach / peak_issue, "traffic": DRAM_BYTES_PER_LAUNCH,
+                "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz {sm_mhz:.0f} "
+                               f"(MEASURED_PEAKS.json, {kind})",
+                "ops_per_placement": REF_OPS_PER_PLACEMENT,
+                "ops_basis": "reference algorithm per-placement operation count (DESIGN.md section 6)",
+                "lane_instr_per_placement_measured": LANE_INSTR_PER_PLACEMENT,
+                "issue_frac_measured": per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12 / peak_issue}
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = host_threads()

@@ -1,0 +1,86 @@
+// ta3b.hpp -- header-only C++ drop-in for ta3::gpu::ModelEvaluator over the C ABI (ta3b.h).
+//
+// Same class name, member signatures, argument meaning and error behaviour
+// (std::runtime_error) as the reference's ta3_gpu/incl/ta3/gpu/model_eval.hpp:27-114, so
+// ta3_trainer's TetrisProblem2::evalBatch (ta3_trainer/src/tetris_problem2.cpp:44-72) compiles
+// against it unchanged. eval_host (the CPU parity path) is not provided: the product has no CPU
+// evaluator; parity tooling lives in the repository's oracle/.
+#pragma once
+#include "ta3b.h"
+
+#include <cstdint>
+#include <memory>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace ta3::gpu {
+
+using weights_t = float;
+
+class ModelEvaluator {
+public:
+    explicit ModelEvaluator(int device = 0) {
+        ta3b_config const cfg{device, 0, 0};
+        _ctx.reset(ta3b_create(&cfg));
+        if (!_ctx) throw std::runtime_error(std::string("ta3b: ") + ta3b_last_error(nullptr));
+    }
+
+    // model_eval.hpp:46-51: per-(model, game) fitness, model-major
+    [[nodiscard]] std::vector<float> eval(std::span<weights_t const> weights, std::uint32_t num_models,
+                                          std::span<std::uint64_t const> seeds, std::uint32_t max_moves) {
+        std::vector<float> out(static_cast<std::size_t>(num_models) * seeds.size());
+        if (weights.size() != static_cast<std::size_t>(num_models) * TA3B_NUM_PARAMS)
+            throw std::runtime_error("ta3b: eval: weights.size() must equal num_models * NUM_PARAMS");
+        check(ta3b_eval(_ctx.get(), weights.data(), num_models, TA3B_NUM_PARAMS, seeds.data(),
+                        static_cast<std::uint32_t>(seeds.size()), max_moves, out.data(), nullptr, nullptr));
+        return out;
+    }
+
+    // model_eval.hpp:54-59: single-model convenience
+    [[nodiscard]] std::vector<float> eval(std::span<weights_t const> weights, std::span<std::uint64_t const> seeds,
+                                          std::uint32_t max_moves) {
+        return eval(weights, 1u, seeds, max_moves);
+    }
+
+    // extension: scores plus piece and line counts in one call
+    void eval_full(std::span<weights_t const> weights, std::uint32_t num_models, std::span<std::uint64_t const> seeds,
+                   std::uint32_t max_moves, std::vector<float>& score, std::vector<std::uint32_t>& pieces,
+                   std::vector<std::uint32_t>& lines) {
+        std::size_t const n = static_cast<std::size_t>(num_models) * seeds.size();
+        score.resize(n);
+        pieces.resize(n);
+        lines.resize(n);
+        check(ta3b_eval(_ctx.get(), weights.data(), num_models, static_cast<std::uint32_t>(
+                            num_models ? weights.size() / num_models : TA3B_NUM_PARAMS),
+                        seeds.data(), static_cast<std::uint32_t>(seeds.size()), max_moves, score.data(),
+                        pieces.data(), lines.data()));
+    }
+
+private:
+    void check(int rc) const {
+        if (rc != TA3B_OK) throw std::runtime_error(std::string("ta3b: ") + ta3b_last_error(_ctx.get()));
+    }
+    struct Deleter {
+        void operator()(ta3b_ctx* c) const { ta3b_destroy(c); }
+    };
+    std::unique_ptr<ta3b_ctx, Deleter> _ctx;
+};
+
+// model_eval.hpp:84-103: games seeds drawn from xoshiro256**(seed), shared by every model
+inline std::vector<float> simulate(ModelEvaluator& evaluator, std::span<weights_t const> model_weights,
+                                   std::size_t num_models, std::size_t games, std::uint64_t seed,
+                                   std::size_t max_moves) {
+    std::vector<std::uint64_t> seeds(games);
+    ta3b_simulate_seeds(seed, static_cast<std::uint32_t>(games), seeds.data());
+    return evaluator.eval(model_weights, static_cast<std::uint32_t>(num_models), seeds,
+                          static_cast<std::uint32_t>(max_moves));
+}
+
+inline std::vector<float> simulate(ModelEvaluator& evaluator, std::span<weights_t const> model_weights,
+                                   std::size_t games, std::uint64_t seed, std::size_t max_moves) {
+    return simulate(evaluator, model_weights, 1, games, seed, max_moves);
+}
+
+} // namespace ta3::gpu

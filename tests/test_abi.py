@@ -1,0 +1,101 @@
+"""The C-ABI library without a GPU: it loads, exports every function
+include/ta3b.h declares, its host-only seed derivation equals the reference's,
+the C++ drop-in header compiles and links against it, and without a device it
+fails loudly (there is no CPU fallback)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+import shutil
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden, ptr
+
+HEADER = os.path.join(ROOT, "include", "ta3b.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(ta3b_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from tetris_ai3_b200 import library
+    return library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_functions()
+    assert len(names) >= 12
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_the_header():
+    from tetris_ai3_b200.evaluator import EXPORTS
+    assert sorted(EXPORTS) == declared_functions()
+
+
+def test_simulate_seeds_match_reference(lib):
+    g = load_golden("engine")["simulate_seeds"]
+    for s, want in g.items():
+        out = np.zeros(16, np.uint64)
+        assert lib.ta3b_simulate_seeds(C.c_uint64(int(s)), 16, ptr(out)) == 0
+        assert [str(int(v)) for v in out] == want
+    from tetris_ai3_b200 import simulate_seeds, workload
+    assert np.array_equal(simulate_seeds(42, 16), workload.xoshiro_seeds(42, 16))
+
+
+def test_variants_enumerate(lib):
+    from tetris_ai3_b200 import ModelEvaluator
+    v = ModelEvaluator.variants()
+    assert len(v) == lib.ta3b_num_variants() >= 2
+    assert all(x["warps_per_block"] in (2, 4) for x in v)
+
+
+def _has_gpu():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.mark.skipif(_has_gpu(), reason="checks the no-device error path")
+def test_fails_loudly_without_a_device():
+    from tetris_ai3_b200 import EvaluatorError, ModelEvaluator
+    with pytest.raises(EvaluatorError):
+        ModelEvaluator(device=0)
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_cpp_dropin_header_compiles_and_links(tmp_path):
+    src = tmp_path / "use.cpp"
+    src.write_text(r'''
+#include <ta3b.hpp>
+#include <cstdio>
+int main() {
+    std::vector<float> w(97, 0.1f);
+    std::vector<std::uint64_t> seeds{1, 2};
+    try {
+        ta3::gpu::ModelEvaluator ev;
+        auto s = ta3::gpu::simulate(ev, w, 2, 7, 300);
+        std::printf("ran %zu\n", s.size());
+    } catch (std::runtime_error const& e) {
+        std::printf("error %s\n", e.what());
+    }
+    return 0;
+}
+''')
+    exe = tmp_path / "use"
+    libdir = os.path.join(ROOT, "tetris_ai3_b200", "_lib")
+    subprocess.run(["g++", "-std=c++20", "-I", os.path.join(ROOT, "include"), str(src), "-L", libdir, "-lta3b",
+                    f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout
+    assert out.startswith("ran 7") if _has_gpu() else out.startswith("error ta3b:")
