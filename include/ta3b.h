@@ -86,6 +86,26 @@ int ta3b_eval_device(ta3b_ctx* ctx, const float* d_weights, uint32_t num_islands
                      uint32_t num_params, const uint64_t* d_seeds, uint32_t num_games, uint32_t max_moves,
                      float* d_score, uint32_t* d_pieces, uint32_t* d_lines, uint32_t* d_evals, void* stream);
 
+/* Allocation-free variant of ta3b_eval_device, for callers that must not call
+ * cudaMalloc where they evaluate (a host framework whose pooling allocator owns
+ * all device memory; a scheduler thread that cannot afford cudaMalloc's implicit
+ * device synchronisation). No context: pass device inputs and outputs and a
+ * stream (NULL = legacy default stream); nothing is allocated. The kernel's only
+ * scratch -- its work-queue ticket and error status -- is a 256-byte static
+ * device array that every GPU loading this library keeps until exit. The first
+ * call on each device sets that device up (resolves the array's address,
+ * configures the kernel) with the device current; make that first call before
+ * any stream capture. Every call shares the one array and clears it on entry,
+ * so calls whose kernels overlap on the GPU race: run them on one stream or
+ * serialise them. A call may cover at most 2^32 - 65 sims; larger batches,
+ * num_params != 97 and null pointers are rejected with TA3B_ERR_ARG and, when
+ * error_out is not NULL, a static message in *error_out. Enqueued, not
+ * synchronised. No counterpart in the reference. */
+int ta3b_eval_device_noalloc(const float* d_weights, uint32_t num_islands, uint32_t models_per_island,
+                             uint32_t num_params, const uint64_t* d_seeds, uint32_t num_games, uint32_t max_moves,
+                             float* d_score, uint32_t* d_pieces, uint32_t* d_lines, uint32_t* d_evals,
+                             void* stream, const char** error_out);
+
 /* Per-move trace of every sim (debug / parity tooling): trace_out receives
  * 3 bytes per move (hold, orientation, x + 2), max_moves moves per sim,
  * model-major; n_moves_out the number of searched moves per sim;

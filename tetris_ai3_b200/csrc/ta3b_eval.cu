@@ -27,6 +27,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 namespace ta3b {
@@ -1147,3 +1148,95 @@ int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_bl
 }
 
 } // extern "C"
+
+// ============================================ allocation-free evaluation ===
+// Some hosts cannot call cudaMalloc where they evaluate: a framework whose own
+// pooling allocator owns all device memory (raw cudaMalloc/cudaFree calls
+// bypass its accounting and can fragment or exhaust its pool), or a latency-
+// critical scheduler thread that must not pay cudaMalloc/cudaFree's implicit
+// device-wide synchronisation. ta3b_eval_device_noalloc serves them: it creates
+// no context and allocates nothing. The caller passes device inputs and
+// outputs; the only scratch the evaluation kernel needs -- its work-queue
+// ticket and error status word -- lives in the file-scope array below, which
+// every GPU that loads this library holds until the process exits.
+namespace {
+
+constexpr uint32_t kNoAllocScratchWords = 64;                 // 256 bytes; words 0 (ticket) and 1 (status) used
+constexpr uint64_t kNoAllocMaxSims = 0xFFFFFFFFull - 64u;     // the 32-bit ticket must not wrap
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocScratchWords];
+
+constexpr int kNoAllocMaxDevices = 64;
+struct NoAllocDevice {
+    uint32_t* scratch;   // device address of g_noalloc_scratch on this device
+    uint32_t grid;
+    bool ready;
+};
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+std::mutex g_noalloc_mu;
+
+} // namespace
+
+extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_islands, uint32_t models_per_island,
+                                        uint32_t num_params, uint64_t const* d_seeds, uint32_t num_games,
+                                        uint32_t max_moves, float* d_score, uint32_t* d_pieces, uint32_t* d_lines,
+                                        uint32_t* d_evals, void* stream, char const** error_out) {
+    auto fail_static = [&](int code, char const* msg) {
+        if (error_out) *error_out = msg;
+        return code;
+    };
+    if (error_out) *error_out = "";
+    if (num_params != NPARAMS) return fail_static(TA3B_ERR_ARG, "num_params must be 97 (v11 value model)");
+    uint64_t const sims = uint64_t(num_islands) * models_per_island * num_games;
+    if (sims > kNoAllocMaxSims)
+        return fail_static(TA3B_ERR_ARG, "too many sims for the allocation-free path (at most 2^32 - 65 per call)");
+    if (sims == 0) return TA3B_OK;
+    if (!d_weights || !d_seeds || !d_score) return fail_static(TA3B_ERR_ARG, "null device pointer");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail_static(TA3B_ERR_CUDA, "cudaGetDevice failed or device ordinal too large");
+    Variant const& var = kVariants[kDefaultVariant];
+    size_t const dyn = var.warps * sizeof(WarpShared);
+    {
+        // once per device, with that device current: resolve the scratch array's
+        // device address (its host-side name is only a stand-in) and set the
+        // kernel's shared-memory limit
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        NoAllocDevice& d = g_noalloc_dev[dev];
+        if (!d.ready) {
+            void* ptr = nullptr;
+            if (cudaGetSymbolAddress(&ptr, g_noalloc_scratch) != cudaSuccess || !ptr)
+                return fail_static(TA3B_ERR_CUDA, "cudaGetSymbolAddress of the scratch array failed");
+            if (cudaFuncSetAttribute(var.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)) != cudaSuccess)
+                return fail_static(TA3B_ERR_CUDA, "cudaFuncSetAttribute failed");
+            int sms = 0, per_sm = 0;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, var.fn, int(var.warps * 32), dyn) != cudaSuccess ||
+                per_sm < 1)
+                return fail_static(TA3B_ERR_CUDA, "occupancy query failed");
+            d.scratch = static_cast<uint32_t*>(ptr);
+            d.grid = uint32_t(sms) * uint32_t(per_sm);
+            d.ready = true;
+        }
+    }
+    NoAllocDevice const& d = g_noalloc_dev[dev];
+    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+    // the array keeps the previous call's contents: the ticket and status must start at zero
+    if (cudaMemsetAsync(d.scratch, 0, 2 * sizeof(uint32_t), st) != cudaSuccess)
+        return fail_static(TA3B_ERR_CUDA, "clearing the scratch array failed");
+    Params prm{};
+    prm.weights = d_weights;
+    prm.seeds = d_seeds;
+    prm.score = d_score;
+    prm.pieces = d_pieces;
+    prm.lines = d_lines;
+    prm.evals = d_evals;
+    prm.scratch = d.scratch;
+    prm.num_games = num_games;
+    prm.models_per_island = models_per_island;
+    prm.max_moves = max_moves;
+    prm.total_sims = uint32_t(sims);
+    uint32_t const need = uint32_t((sims + var.warps - 1) / var.warps);
+    var.fn<<<need < d.grid ? need : d.grid, var.warps * 32, dyn, st>>>(prm);
+    if (cudaGetLastError() != cudaSuccess) return fail_static(TA3B_ERR_CUDA, "kernel launch failed");
+    return TA3B_OK;
+}

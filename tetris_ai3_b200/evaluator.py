@@ -23,7 +23,7 @@ _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
            "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
-           "ta3b_select_variant", "ta3b_core_selftest"]
+           "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc"]
 
 
 class EvaluatorError(RuntimeError):
@@ -60,6 +60,8 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_variant_info.argtypes = [C.c_int, vp, vp]
     lib.ta3b_select_variant.argtypes = [vp, C.c_int]
     lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
+    lib.ta3b_eval_device_noalloc.argtypes = [vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp,
+                                             C.POINTER(C.c_char_p)]
     if path is None:
         _lib = lib
     return lib
