@@ -1,6 +1,6 @@
 """Benchmark: beam placements/s of one CMA-ES generation's evaluation on B200.
 
-One step = one generation of configs[1]: 4 islands x 50 candidates x 50 games =
+One step = one CMA-ES generation: 4 islands x 50 candidates x 50 games =
 10,000 (model, game) sims, v11 weights, cap 2,000 pieces, every game played
 with the depth-4 beam (16/32/32) to the cap or top-out. The unit is the
 evaluated beam placement (one value-model call inside search_move_beam), an
@@ -36,7 +36,7 @@ sys.path.insert(0, ROOT)
 
 from tetris_ai3_b200 import workload  # noqa: E402
 
-METRIC = "beam placements/s on 1 B200 (configs[1]: one CMA-ES generation, 10k sims, cap 2000)"
+METRIC = "beam placements/s on 1 B200 (one CMA-ES generation: 4 islands x 50 models x 50 games = 10k sims, cap 2000)"
 UNIT = "placements/s"
 # Issue roofline (the path is INT32/FP32 issue-bound, not HBM- or tensor-bound):
 # REF_OPS_PER_PLACEMENT is the reference algorithm's operation count for one
@@ -46,15 +46,13 @@ UNIT = "placements/s"
 # (192); key (6) = 1010.
 REF_OPS_PER_PLACEMENT = 1010
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
-# profiles/eval_kernel_small_case_full.md) and its DRAM bytes per configs[1] launch
-# (ncu dram__bytes_read.sum + dram__bytes_write.sum, profiles/eval_kernel_configs1_launches.md).
+# on the small-case capture) and its DRAM bytes per full-generation launch
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum).
 LANE_INSTR_PER_PLACEMENT = 564
 DRAM_BYTES_PER_LAUNCH = None
 
 
-def _dist_env():
-    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), \
-        int(os.environ.get("LOCAL_RANK", "0"))
+from tetris_ai3_b200.dist import rank_env as _dist_env, rank_seed, reduce_timing  # noqa: E402
 
 
 def _peaks():
@@ -162,7 +160,7 @@ def run_reference(args):
     rank, world, _ = _dist_env()
     if rank != 0:
         return
-    batch = workload.config1()
+    batch = workload.generation_batch()
     threads = host_threads()
     rates = []
     kind = "reference"
@@ -171,7 +169,7 @@ def run_reference(args):
         r, kind, sims, t = cpu_rate(batch, budget_s=args.ref_budget, threads=threads)
         if step >= args.warmup:
             rates.append(r)
-            sample_desc = f"first {sims} sims of configs[1] (island 0, model-major), cap 2000, {t:.1f} s per step"
+            sample_desc = f"first {sims} sims of the generation (island 0, model-major), cap 2000, {t:.1f} s per step"
     v = float(np.mean(rates))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
@@ -205,7 +203,8 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     # weak scaling: each rank scores its own generation (islands seeded per rank)
-    batch = workload.config1(islands=args.islands, pop=args.pop, games=args.games, max_moves=args.cap, seed=1 + rank)
+    batch = workload.generation_batch(islands=args.islands, pop=args.pop, games=args.games, max_moves=args.cap,
+                             seed=rank_seed(1, rank))
     ev = ModelEvaluator(device=local)
     stream = torch.cuda.Stream(device=dev)
     w_dev = torch.from_numpy(batch.weights).to(dev)
@@ -252,16 +251,7 @@ def run_ours(args):
     torch.cuda.synchronize()
     clocks = clk.summary()
     t_local = sum(ms) / 1000.0
-    t_max = t_local
-    total_pl = placements
-    if world > 1:
-        tt = torch.tensor([t_local], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        pt = torch.tensor([placements], device=dev, dtype=torch.float64)
-        dist.all_reduce(pt, op=dist.ReduceOp.SUM)
-        total_pl = int(pt.item())
-    value = total_pl / t_max
+    t_max, total_pl, value = reduce_timing(t_local, float(placements), dev)
 
     # ---- end to end through the public API: pinned host buffers in, host results out
     h_w = torch.from_numpy(batch.weights).pin_memory()
@@ -281,11 +271,7 @@ def run_ours(args):
                                    batch.games, batch.max_moves, vp(h_sc), vp(h_pc), vp(h_lc))
         if rc:
             raise RuntimeError(lib.ta3b_last_error(ev._ctx).decode())
-    e2e_t = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_t], device=dev, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
+    e2e_t, _, _ = reduce_timing(time.perf_counter() - t0, 0.0, dev)
     assert h_sc.numpy().tobytes() == score.cpu().numpy().tobytes(), "e2e results differ from the device run"
     e2e_value = (total_pl / args.steps) * e2e_steps / e2e_t
     h2d = batch.weights.nbytes + batch.seeds.nbytes
@@ -303,7 +289,7 @@ def run_ours(args):
                 "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz {sm_mhz:.0f} "
                                f"(MEASURED_PEAKS.json, {kind})",
                 "ops_per_placement": REF_OPS_PER_PLACEMENT,
-                "ops_basis": "reference algorithm per-placement operation count (DESIGN.md section 6)",
+                "ops_basis": "reference algorithm per-placement operation count (hand count above)",
                 "lane_instr_per_placement_measured": LANE_INSTR_PER_PLACEMENT,
                 "issue_frac_measured": per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12 / peak_issue}
         cpu = None
@@ -311,7 +297,7 @@ def run_ours(args):
             threads = host_threads()
             r, ck, sims, t = cpu_rate(batch, budget_s=args.cpu_budget, threads=threads)
             cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": ck,
-                   "sample": f"first {sims} sims of configs[1] (island 0, model-major), cap 2000, {t:.1f} s"}
+                   "sample": f"first {sims} sims of the generation (island 0, model-major), cap 2000, {t:.1f} s"}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "fp32+int32", "data": "synthetic",
@@ -342,7 +328,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="fixed kernel variant (default: autotune)")
     ap.add_argument("--no-autotune", action="store_true")
-    # reduced shapes for profiling captures only (the headline is the default configs[1])
+    # reduced shapes for profiling captures only (the headline is the default full generation)
     ap.add_argument("--islands", type=int, default=4)
     ap.add_argument("--pop", type=int, default=50)
     ap.add_argument("--games", type=int, default=50)

@@ -153,8 +153,8 @@ def games():
                       "max_moves": cap, "results": res})
         print(name, [[r["pieces"] for r in row] for row in res], flush=True)
 
-    c0 = workload.config0()
-    add("config0: N(0,0.5^2) seed 0, seeds 0..7, cap 500", c0.weights, c0.seeds[0], 500)
+    c0 = workload.single_model_batch()
+    add("single model: N(0,0.5^2) seed 0, seeds 0..7, cap 500", c0.weights, c0.seeds[0], 500)
     pw = np.zeros(P, np.float32)
     for ms in (11, 22, 33):                                  # parity_test.cpp:51-66
         REF.ta3ref_parity_weights(ms, ptr(pw))

@@ -40,9 +40,9 @@ def test_golden_games_bit_exact(ev, golden_games):
         _check_golden_case(ev, case)
 
 
-def test_config0_matches_golden(ev, golden_games):
+def test_single_model_matches_golden(ev, golden_games):
     from tetris_ai3_b200 import workload
-    b = workload.config0()
+    b = workload.single_model_batch()
     case = golden_games["cases"][0]
     assert np.array_equal(weights_from_hex(case["weights"]), b.weights)
     sc, pc, lc = ev.eval_full(b.weights, 1, b.seeds[0], b.max_moves)
@@ -78,7 +78,7 @@ def test_random_models_match_oracle(ev, oracle):
 
 def test_islands_equal_separate_calls(ev):
     from tetris_ai3_b200 import workload
-    b = workload.config1(islands=3, pop=4, games=5, max_moves=120, seed=9)
+    b = workload.generation_batch(islands=3, pop=4, games=5, max_moves=120, seed=9)
     sc, pc, lc = ev.eval_islands(b.weights, b.seeds, b.max_moves)
     for i in range(3):
         s2, p2, l2 = ev.eval_full(b.weights[i * 4:(i + 1) * 4], 4, b.seeds[i], b.max_moves)
@@ -117,10 +117,10 @@ def test_extreme_weights_match_oracle(ev, oracle):
     assert sc.tobytes() == osc.tobytes() and np.array_equal(pc, opc) and np.array_equal(lc, olc)
 
 
-def test_full_config1_properties(ev, oracle):
-    # configs[1] at full size: deterministic, island-consistent, and a sample matches the oracle
+def test_full_generation_properties(ev, oracle):
+    # the full generation (4 x 50 models x 50 games, cap 2000): deterministic, island-consistent, and a sample matches the oracle
     from tetris_ai3_b200 import workload
-    b = workload.config1()
+    b = workload.generation_batch()
     sc1, pc1, lc1 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
     sc2, pc2, lc2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
     assert sc1.tobytes() == sc2.tobytes() and np.array_equal(pc1, pc2)
@@ -179,3 +179,17 @@ def test_device_core_matches_host_core(ev):
     packed_bad = int(((fs == 0) & (dd[:, 31].view(np.uint32) != fv.view(np.uint32))).sum())
     print("packed f32x2 MLP mismatches:", packed_bad, "of", int((fs == 0).sum()))
     assert not mism, f"{len(mism)} of {n} candidates differ"
+
+
+def test_generation_graph_replays_match_direct_calls(ev):
+    """The per-generation CUDA graph (pinned H2D, kernel, D2H) gives the direct
+    call's results, and replays correctly with new populations."""
+    from tetris_ai3_b200 import workload
+    from tetris_ai3_b200.evaluator import GenerationGraph
+    g = GenerationGraph(ev, models=8, islands=2, games=6, max_moves=140)
+    for seed in (31, 32):
+        b = workload.generation_batch(islands=2, pop=4, games=6, max_moves=140, seed=seed)
+        sc, pc, lc, ec = g.run(b.weights, b.seeds)
+        s2, p2, l2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+        assert sc.tobytes() == s2.tobytes() and np.array_equal(pc, p2) and np.array_equal(lc, l2)
+        assert (ec > 0).all()

@@ -28,7 +28,7 @@ def test_noalloc_matches_context_path_twice():
     lib = library()
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    b = workload.config1(islands=2, pop=6, games=8, max_moves=160, seed=21)
+    b = workload.generation_batch(islands=2, pop=6, games=8, max_moves=160, seed=21)
     w = torch.from_numpy(b.weights).to(dev)
     s = torch.from_numpy(b.seeds.view(np.int64)).to(dev)
     n = b.sims

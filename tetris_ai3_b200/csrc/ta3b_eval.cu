@@ -412,7 +412,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
     uint32_t queued = 0;
     int seg = 0;
     // TA3B_ILP candidates per lane per iteration (c, c+32, ...) in straight-line
-    // code (1 measured fastest on B200: 504 ms per configs[1] step vs 694 ms for 2)
+    // code (1 measured fastest on B200: 504 ms per full-generation step vs 694 ms for 2)
     // code, so their dependency chains interleave; out-of-range slots evaluate
     // the last real candidate and are discarded
     for (uint32_t c0 = 0; c0 < total; c0 += TA3B_ILP * WARP) {
@@ -747,7 +747,7 @@ Variant const kVariants[] = {
     {eval_kernel<2, 10>, 2, 10}, {eval_kernel<2, 12>, 2, 12},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
-constexpr int kDefaultVariant = 1;   // 4 warps, 4 blocks/SM: fastest on configs[1] in every autotune run
+constexpr int kDefaultVariant = 1;   // 4 warps, 4 blocks/SM: fastest on the full generation in every autotune run
 
 } // namespace
 } // namespace ta3b

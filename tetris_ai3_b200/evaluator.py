@@ -225,3 +225,53 @@ def simulate(evaluator: ModelEvaluator, model_weights, num_models: int, games: i
              max_moves: int) -> np.ndarray:
     """ta3::gpu::simulate: games seeds drawn from xoshiro256**(seed), shared by every model."""
     return evaluator.eval(model_weights, num_models, simulate_seeds(seed, games), max_moves)
+
+
+class GenerationGraph:
+    """One CMA-ES generation's launch sequence captured as a CUDA graph:
+    pinned host weights and seeds -> device, the evaluation kernel (work-queue
+    reset + persistent launch), device results -> pinned host. Replaying it
+    scores a new population of the same shape with one graph launch."""
+
+    def __init__(self, evaluator: ModelEvaluator, models: int, islands: int, games: int, max_moves: int,
+                 device: int = 0):
+        import torch
+        if models % islands:
+            raise EvaluatorError("model count must be a multiple of the island count")
+        self.torch = torch
+        dev = torch.device("cuda", device)
+        self.shape = (models, islands, games, max_moves)
+        n = models * games
+        self.h_w = torch.empty((models, NUM_PARAMS), dtype=torch.float32).pin_memory()
+        self.h_s = torch.empty((islands, games), dtype=torch.int64).pin_memory()
+        self.d_w = torch.empty((models, NUM_PARAMS), dtype=torch.float32, device=dev)
+        self.d_s = torch.empty((islands, games), dtype=torch.int64, device=dev)
+        self.d_out = [torch.empty(n, dtype=t, device=dev) for t in (torch.float32, torch.int32, torch.int32,
+                                                                     torch.int32)]
+        self.h_out = [torch.empty(n, dtype=t).pin_memory() for t in (torch.float32, torch.int32, torch.int32,
+                                                                      torch.int32)]
+        self.stream = torch.cuda.Stream(device=dev)
+        self.graph = torch.cuda.CUDAGraph()
+        self.h_w.zero_()
+        self.h_s.zero_()
+        with torch.cuda.graph(self.graph, stream=self.stream):
+            self.d_w.copy_(self.h_w, non_blocking=True)
+            self.d_s.copy_(self.h_s, non_blocking=True)
+            evaluator.eval_device(self.d_w, self.d_s, max_moves, *self.d_out, num_islands=islands,
+                                  stream=self.stream)
+            for h, d in zip(self.h_out, self.d_out):
+                h.copy_(d, non_blocking=True)
+
+    def run(self, weights, seeds_per_island):
+        """Score one population: (score, pieces, lines, evaluated placements), model-major."""
+        models, islands, games, _ = self.shape
+        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(models, NUM_PARAMS)
+        s = np.ascontiguousarray(seeds_per_island, dtype=np.uint64).reshape(islands, games)
+        self.h_w.numpy()[:] = w
+        self.h_s.numpy()[:] = s.view(np.int64)
+        # replay() launches on the current stream: make that the stream whose completion we wait for
+        with self.torch.cuda.stream(self.stream):
+            self.graph.replay()
+        self.stream.synchronize()
+        sc, pc, lc, ec = (h.numpy().copy() for h in self.h_out)
+        return sc, pc.view(np.uint32), lc.view(np.uint32), ec.view(np.uint32)

@@ -1,4 +1,4 @@
-"""Per-sim scheduling profile of one configs[1] generation on the GPU:
+"""Per-sim scheduling profile of one full generation (4 islands x 50 models x 50 games, cap 2000) on the GPU:
 records when each sim started and finished and how many placements it
 evaluated, and writes them to an .npz for analysis of the launch tail.
 
@@ -18,7 +18,7 @@ def main():
     ap.add_argument("--out", required=True)
     ap.add_argument("--variant", type=int, default=-1)
     args = ap.parse_args()
-    b = workload.config1()
+    b = workload.generation_batch()
     ev = ModelEvaluator()
     if args.variant >= 0:
         ev.select_variant(args.variant)

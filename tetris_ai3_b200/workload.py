@@ -10,7 +10,7 @@ machine builds the same inputs for the same config:
   to [0, 1) with 53 bits.
 * ``normal(seed, n)`` -- Box-Muller in float64 over consecutive uniform pairs.
 
-Game seeds follow the reference: either given directly (configs[0] uses 0..7)
+Game seeds follow the reference: either given directly (the 1-model x 8-game case uses 0..7)
 or derived like ``ta3::gpu::simulate`` (ta3_gpu/incl/ta3/gpu/model_eval.hpp:148-151):
 xoshiro256**(seed) draws, one per game.
 """
@@ -121,13 +121,13 @@ class Batch:
         return self.models * self.games
 
 
-def config0() -> Batch:
+def single_model_batch() -> Batch:
     """1 v11 model, weights N(0, 0.5^2) from seed 0, games with seeds 0..7, cap 500."""
     w = (0.5 * normal(0, NUM_PARAMS)).astype(np.float32)[None, :]
-    return Batch("c0: 1 model x 8 games, cap 500", w, np.arange(8, dtype=np.uint64)[None, :], 500)
+    return Batch("1 model x 8 games, cap 500", w, np.arange(8, dtype=np.uint64)[None, :], 500)
 
 
-def config1(islands: int = 4, pop: int = 50, games: int = 50, max_moves: int = 2000, seed: int = 1) -> Batch:
+def generation_batch(islands: int = 4, pop: int = 50, games: int = 50, max_moves: int = 2000, seed: int = 1) -> Batch:
     """One CMA-ES generation: islands x pop candidates x games. Island mean
     m ~ N(0, 0.25) (variance 0.25) from ``seed``; candidates N(m, 0.5^2 I);
     island i plays the ``games`` seeds simulate() derives from seed*1000+i."""
@@ -135,11 +135,11 @@ def config1(islands: int = 4, pop: int = 50, games: int = 50, max_moves: int = 2
     z = normal(seed + 0x51ED, islands * pop * NUM_PARAMS).reshape(islands * pop, NUM_PARAMS)
     w = (m[None, :] + 0.5 * z).astype(np.float32)
     seeds = np.stack([xoshiro_seeds(seed * 1000 + i, games) for i in range(islands)])
-    return Batch(f"c1: {islands} islands x {pop} x {games} games = {islands * pop * games} sims, cap {max_moves}",
+    return Batch(f"{islands} islands x {pop} x {games} games = {islands * pop * games} sims, cap {max_moves}",
                  w, seeds, max_moves)
 
 
-def config2(models: int = 200, games: int = 100, max_moves: int = 10000, seed: int = 2) -> Batch:
+def uneven_batch(models: int = 200, games: int = 100, max_moves: int = 10000, seed: int = 2) -> Batch:
     """Uneven lengths: 10 % of the models are the shipped v11 champion, 90 %
     N(0, 1) weights, order shuffled by ``seed``; one island."""
     n_champ = models // 10
@@ -147,4 +147,4 @@ def config2(models: int = 200, games: int = 100, max_moves: int = 10000, seed: i
     w = np.concatenate([np.repeat(champion()[None, :], n_champ, axis=0), rnd]).astype(np.float32)
     order = np.argsort(splitmix_u64(seed + 7, models), kind="stable")
     seeds = xoshiro_seeds(seed, games)[None, :]
-    return Batch(f"c2: {models} models x {games} games (10% champion), cap {max_moves}", w[order], seeds, max_moves)
+    return Batch(f"{models} models x {games} games (10% champion), cap {max_moves}", w[order], seeds, max_moves)
