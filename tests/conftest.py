@@ -69,3 +69,18 @@ def oracle_eval(lib, w: np.ndarray, seeds: np.ndarray, max_moves: int, threads: 
     lib.ta3o_eval_mt(ptr(w), w.shape[0], ptr(seeds), seeds.size, max_moves, threads, ptr(sc), ptr(pc), ptr(lc),
                      C.byref(ev))
     return sc, pc, lc, ev.value
+
+
+HOST_SO = os.path.join(ROOT, "tetris_ai3_b200", "_lib", "libta3b_host.so")
+
+
+@pytest.fixture(scope="session")
+def host():
+    """The C++ host library (CMA-ES + island trainer), built if absent."""
+    if not os.path.exists(HOST_SO):
+        from tetris_ai3_b200 import build as b
+        if not os.path.exists(b.LIB):
+            b.build_lib()
+        b.build_host()
+    from tetris_ai3_b200 import trainer
+    return trainer

@@ -99,3 +99,53 @@ int main() {
                     f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout
     assert out.startswith("ran 7") if _has_gpu() else out.startswith("error ta3b:")
+
+
+def _declared(header: str, prefix: str):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(rf"\b({prefix}[a-z0-9_]+)\s*\(", text)) - {"ta3t_score_fn"})
+
+
+def test_host_library_exports_the_cma_and_trainer_headers(host):
+    lib = host.host_library()
+    names = _declared("ta3b_cma.h", "ta3c_") + _declared("ta3b_trainer.h", "ta3t_")
+    assert len(names) >= 25
+    assert [n for n in names if not hasattr(lib, n)] == []
+    assert sorted(host.HOST_EXPORTS) == names
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="needs g++")
+def test_cpp_trainer_headers_compile_and_link(tmp_path):
+    src = tmp_path / "use_trainer.cpp"
+    src.write_text(r'''
+#include <ta3b_cma.h>
+#include <ta3b_trainer.h>
+#include <cstdio>
+#include <vector>
+static int score(void*, const float* w, uint32_t n, uint32_t p, const uint64_t*, uint32_t g, uint32_t,
+                 float* out, uint32_t*) {
+    for (uint32_t m = 0; m < n; ++m) {
+        double s = 0; for (uint32_t j = 0; j < p; ++j) s -= double(w[m * p + j]) * w[m * p + j];
+        for (uint32_t k = 0; k < g; ++k) out[m * g + k] = float(s);
+    }
+    return 0;
+}
+int main() {
+    ta3t_config c; ta3t_default_config(&c);
+    c.islands = 2; c.population = 6; c.games = 2; c.gens_per_iteration = 2;
+    ta3t_trainer* t = ta3t_create(&c, score, nullptr, nullptr);
+    if (!t) { std::printf("error %s\n", ta3t_last_error(nullptr)); return 1; }
+    ta3t_run(t, 2);
+    ta3t_stats st; ta3t_get_stats(t, &st);
+    std::printf("gens %llu\n", (unsigned long long)st.generation);
+    ta3t_destroy(t);
+    return 0;
+}
+''')
+    exe = tmp_path / "use_trainer"
+    libdir = os.path.join(ROOT, "tetris_ai3_b200", "_lib")
+    subprocess.run(["g++", "-std=c++20", "-I", os.path.join(ROOT, "include"), str(src), "-L", libdir, "-lta3b_host",
+                    "-lta3b", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout
+    assert out.startswith("gens 4"), out

@@ -1,0 +1,187 @@
+"""The island CMA-ES trainer (tetris_ai3_b200/host/trainer.cpp) on CPU,
+driven through its score-function hook: lock-step generations (one evaluator
+call per generation for all islands), the reference's seed stream
+(ta3_trainer/src/trainer2.cpp:144-168,316), fitness = -mean score
+(tetris_problem2.cpp:44-72), state and .champ files (trainer2.cpp:213-268),
+and surrogate pre-screening with its Spearman gate."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from conftest import oracle_eval
+
+TARGET = np.linspace(-1.0, 1.0, 97)
+
+
+def quadratic(w, seeds, max_moves):
+    """Higher is better, peak at TARGET; a small per-seed offset keeps games distinct."""
+    base = -((w.astype(np.float64) - TARGET) ** 2).sum(1)
+    return (base[:, None] + (seeds % 5)[None, :] * 0.01).astype(np.float32)
+
+
+def small(host, **kw):
+    cfg = dict(islands=3, population=8, gens_per_iteration=3, iterations_per_cycle=2, games=4, max_moves=50)
+    cfg.update(kw)
+    return host.default_config(**cfg)
+
+
+def test_default_config_is_the_reference_runner(host):
+    c = host.default_config()
+    assert (c.islands, c.population, c.gens_per_iteration, c.iterations_per_cycle) == (4, 50, 10, 10)
+    assert (c.games, c.max_moves, c.algo, c.num_params) == (30, 300, host.DD, 97)
+    assert c.training_seed == 0x3E28DF7B1811145B and c.sigma0 == 1.3 and (c.lower, c.upper) == (-2.0, 2.0)
+
+
+def test_one_evaluator_call_per_generation_for_all_islands(host):
+    t = host.Trainer(small(host), score=quadratic)
+    t.run(2)
+    c = t.cfg
+    n_gens = 2 * c.gens_per_iteration
+    assert t.calls == [(c.islands * c.population, c.games, c.max_moves)] * (1 + n_gens)
+    st = t.stats()
+    assert st["generation"] == n_gens and st["iteration"] == 2
+    assert st["evaluations"] == c.islands * c.population * (1 + n_gens)
+    assert st["sims"] == st["evaluations"] * c.games
+
+
+def test_game_seeds_follow_the_reference_stream(host):
+    from tetris_ai3_b200 import workload
+    seen = []
+
+    def score(w, seeds, mm):
+        seen.append(seeds.copy())
+        return quadratic(w, seeds, mm)
+
+    c = small(host)
+    t = host.Trainer(c, score=score)
+    assert np.array_equal(seen[0], workload.xoshiro_seeds(0, c.games))      # initial populations: seed 0
+    t.run(c.iterations_per_cycle + 1)
+    # draws: archipelago seed, one per island optimiser, then one game seed per cycle
+    draws = workload.xoshiro_seeds(c.training_seed, 1 + c.islands + 2)
+    g1, g2 = int(draws[1 + c.islands]), int(draws[2 + c.islands])
+    per_cycle = c.iterations_per_cycle * c.gens_per_iteration
+    assert all(np.array_equal(s, workload.xoshiro_seeds(g1, c.games)) for s in seen[1:1 + per_cycle])
+    assert np.array_equal(seen[1 + per_cycle], workload.xoshiro_seeds(g2, c.games))
+    assert t.stats()["game_seed"] == g2
+
+
+@pytest.mark.parametrize("algo", [1, 2])
+def test_deterministic_and_improving(host, algo):
+    # sigma0 0.1: the reference's 1.3 spreads samples 5.2 per axis, far outside this quadratic's bowl
+    a = host.Trainer(small(host, algo=algo, sigma0=0.1), score=quadratic)
+    b = host.Trainer(small(host, algo=algo, sigma0=0.1), score=quadratic)
+    f0 = a.stats()["best_fitness"]
+    a.run(4)
+    b.run(4)
+    for i in range(3):
+        xa, fa = a.champion(i)
+        xb, fb = b.champion(i)
+        assert fa == fb and np.array_equal(xa, xb)
+        assert np.array_equal(a.island_mean(i), b.island_mean(i))
+    assert a.stats()["best_fitness"] < f0
+
+
+def test_fitness_is_minus_the_mean_oracle_score(host, oracle):
+    c = small(host, islands=2, population=6, games=3, max_moves=40)
+
+    def score(w, seeds, mm):
+        sc, pc, _, _ = oracle_eval(oracle, w, seeds, mm)
+        return sc.reshape(len(w), -1), pc.reshape(len(w), -1)
+
+    t = host.Trainer(c, score=score)
+    t.run_generation()                              # still game seed 0
+    from tetris_ai3_b200 import workload
+    seeds = workload.xoshiro_seeds(0, c.games)
+    for i in range(c.islands):
+        x, f = t.champion(i)
+        sc, _, _, _ = oracle_eval(oracle, x.astype(np.float32)[None, :], seeds, c.max_moves)
+        assert f == -(sum(float(v) for v in sc) / c.games)
+    assert t.stats()["pieces"] > 0
+
+
+def test_state_and_champ_files(host, tmp_path):
+    c = small(host)
+    t = host.Trainer(c, score=quadratic)
+    t.run(2)
+    path = str(tmp_path / "run.bin")
+    t.save_state(path)
+    champ_path = str(tmp_path / "run.champ")
+    assert os.path.exists(path) and os.path.exists(champ_path)
+    best = min(range(c.islands), key=lambda i: t.champion(i)[1])
+    assert np.array_equal(host.read_champ(champ_path), t.champion(best)[0])
+    # every island of a resumed trainer continues from the saved optimiser
+    r = host.Trainer(c, score=quadratic, state_path=path)
+    for i in range(c.islands):
+        assert np.array_equal(r.island_mean(i), t.island_mean(best))
+    r.run(1)
+    with pytest.raises(RuntimeError):
+        host.Trainer(c, score=quadratic, state_path=str(tmp_path / "missing.bin"))
+
+
+def test_champ_files_round_trip_and_read_the_shipped_champion(host, tmp_path):
+    from tetris_ai3_b200 import workload
+    x = host.read_champ(workload.CHAMPION_PATH)
+    assert x.shape == (97,) and np.array_equal(x.astype(np.float32), workload.champion())
+    p = str(tmp_path / "a.champ")
+    host.write_champ(p, x)
+    assert open(p, "rb").read() == open(workload.CHAMPION_PATH, "rb").read()
+
+
+class Exact:
+    """A surrogate that knows the landscape (rho = 1)."""
+    trains = 0
+
+    def train(self, x, y):
+        self.trains += 1
+        assert x.shape[1] == 97 and len(x) == len(y)
+
+    def predict(self, x):
+        return quadratic(x, np.zeros(1, np.uint64), 0)[:, 0]
+
+
+class Noise(Exact):
+    def predict(self, x):
+        return np.random.default_rng(len(x)).normal(size=len(x))
+
+
+def test_surrogate_prescreens_once_its_rank_correlation_passes(host):
+    c = small(host, surrogate_start_gen=4, surrogate_sample=20, surrogate_top=6, surrogate_random=2,
+               surrogate_retrain=3)
+    sur = Exact()
+    t = host.Trainer(c, score=quadratic, surrogate=sur)
+    for _ in range(9):
+        t.run_generation()
+    sizes = [n for n, _, _ in t.calls]
+    full, pre = c.islands * c.population, c.islands * (6 + 2)
+    assert sizes[:4] == [full] * 4                 # init + generations 1..3
+    assert sizes[4:] == [pre] * 6                  # generations 4..9 pre-screened
+    st = t.stats()
+    assert st["surrogate_active"] == 1 and st["surrogate_trainings"] == 2 and st["last_rho"] > 0.9
+    assert sur.trains == 2
+
+
+def test_surrogate_gate_falls_back_to_full_evaluation(host):
+    c = small(host, surrogate_start_gen=4, surrogate_sample=20, surrogate_top=6, surrogate_random=2,
+               surrogate_retrain=3)
+    t = host.Trainer(c, score=quadratic, surrogate=Noise())
+    for _ in range(7):
+        t.run_generation()
+    full = c.islands * c.population
+    assert [n for n, _, _ in t.calls] == [full] * 8
+    st = t.stats()
+    assert st["surrogate_active"] == 0 and st["last_rho"] < 0.6 and st["surrogate_trainings"] == 2
+
+
+def test_errors_are_reported(host):
+    def broken(w, seeds, mm):
+        raise RuntimeError("no evaluator")
+
+    with pytest.raises(RuntimeError):
+        host.Trainer(small(host), score=broken)
+    with pytest.raises(RuntimeError):
+        host.Trainer(small(host, population=3), score=quadratic)
+    with pytest.raises(RuntimeError):
+        host.Trainer(small(host, surrogate_start_gen=2), score=quadratic)     # no surrogate given

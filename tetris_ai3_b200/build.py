@@ -62,6 +62,26 @@ def build_coretest() -> str:
     return CORETEST_LIB
 
 
+HOSTDIR = os.path.join(PKG, "host")
+HOST_LIB = os.path.join(LIBDIR, "libta3b_host.so")
+HOST_SOURCES = ["cmaes.cpp", "cma_abi.cpp", "trainer.cpp"]
+
+
+def build_host() -> str:
+    """The C++ host side (CMA-ES, island trainer) as libta3b_host.so, linked
+    against libta3b.so (the GPU evaluator) with an $ORIGIN rpath."""
+    os.makedirs(LIBDIR, exist_ok=True)
+    # the system g++ (TA3B_CXX overrides): a CXX wrapper that swaps GCC's
+    # internal paths produced a library whose iostream calls crashed in-process
+    cxx = os.environ.get("TA3B_CXX") or shutil.which("g++") or "g++"
+    srcs = [os.path.join(HOSTDIR, s) for s in HOST_SOURCES]
+    cmd = [cxx, "-std=c++20", "-O2", "-fPIC", "-shared", "-Wall", "-Wextra", "-I", os.path.join(ROOT, "include"),
+           "-o", HOST_LIB + ".tmp", *srcs, "-L", LIBDIR, "-lta3b", "-Wl,-rpath,$ORIGIN", "-pthread"]
+    subprocess.run(cmd, check=True)
+    os.replace(HOST_LIB + ".tmp", HOST_LIB)
+    return HOST_LIB
+
+
 def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
 
@@ -78,6 +98,7 @@ def build_reference_cpu() -> bool:
 
 if __name__ == "__main__":
     log = build_lib(verbose=True)
+    build_host()
     build_coretest()
     build_oracle()
     build_reference_cpu()
