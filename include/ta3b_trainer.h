@@ -67,6 +67,9 @@ typedef struct {
     uint32_t surrogate_random;      /* extra random candidates fully evaluated per island */
     uint32_t surrogate_retrain;     /* retrain period in generations */
     double surrogate_min_rho;       /* Spearman gate on the held-out generation */
+    uint32_t surrogate_epochs;      /* built-in GPU surrogate: epochs per retrain */
+    uint32_t surrogate_batch;       /* built-in GPU surrogate: minibatch rows */
+    double surrogate_lr;            /* built-in GPU surrogate: Adam learning rate */
 } ta3t_config;
 
 typedef struct {
@@ -91,7 +94,8 @@ void ta3t_default_config(ta3t_config* cfg);
 /* Build the archipelago (trainer2.cpp:144-171): islands of uniform random
  * populations, evaluated with game seed 0, optimisers seeded from the training
  * seed's xoshiro256** stream. score_fn NULL: the built-in GPU evaluator
- * (libta3b.so, ta3b_eval on cfg->device). surrogate NULL: no pre-screening.
+ * (libta3b.so, ta3b_eval on cfg->device). surrogate NULL with
+ * surrogate_start_gen > 0: the built-in GPU surrogate (ta3b_surrogate.h).
  * NULL on failure (message via ta3t_last_error(NULL)). */
 ta3t_trainer* ta3t_create(const ta3t_config* cfg, ta3t_score_fn score_fn, void* user, const ta3t_surrogate* surrogate);
 /* Like ta3t_create, but every island's optimiser resumes from a saved state

@@ -149,3 +149,12 @@ int main() {
                     "-lta3b", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout
     assert out.startswith("gens 4"), out
+
+
+def test_surrogate_header_is_exported():
+    from tetris_ai3_b200 import library
+    from tetris_ai3_b200.surrogate import SURROGATE_EXPORTS
+    names = _declared("ta3b_surrogate.h", "ta3s_")
+    assert names == SURROGATE_EXPORTS
+    lib = library()
+    assert [n for n in names if not hasattr(lib, n)] == []

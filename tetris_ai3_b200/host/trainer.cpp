@@ -5,6 +5,7 @@
 
 #include "../../include/ta3b.h"
 #include "../../include/ta3b_cma.h"
+#include "../../include/ta3b_surrogate.h"
 #include "cmaes.hpp"
 
 #include <algorithm>
@@ -96,6 +97,27 @@ double spearman(std::vector<double> const& a, std::vector<double> const& b) {
     return sab / std::sqrt(saa * sbb);
 }
 
+// the built-in surrogate: the GPU MLP behind include/ta3b_surrogate.h
+struct GpuSurrogate {
+    ta3s_model* model = nullptr;
+    uint32_t epochs = 40, batch = 256, trainings = 0;
+    float lr = 1e-3f, weight_decay = 1e-2f;
+    ~GpuSurrogate() {
+        if (model) ta3s_destroy(model);
+    }
+};
+
+int gpu_sur_train(void* user, const float* x, const float* y, uint32_t n, uint32_t) {
+    auto* s = static_cast<GpuSurrogate*>(user);
+    if (ta3s_set_data(s->model, x, y, n)) return 1;
+    float loss = 0.f;
+    return ta3s_train(s->model, s->epochs, s->batch, s->lr, s->weight_decay, 0x5A11u + s->trainings++, &loss);
+}
+
+int gpu_sur_predict(void* user, const float* x, uint32_t n, uint32_t, float* mean_out) {
+    return ta3s_predict(static_cast<GpuSurrogate*>(user)->model, x, n, mean_out, nullptr);
+}
+
 // the built-in score function: the GPU evaluator behind include/ta3b.h
 int gpu_score(void* user, const float* weights, uint32_t num_models, uint32_t num_params, const uint64_t* seeds,
               uint32_t num_games, uint32_t max_moves, float* score_out, uint32_t* pieces_out) {
@@ -132,6 +154,7 @@ struct ta3t_trainer {
     ta3t_score_fn score_fn = nullptr;
     void* user = nullptr;
     ta3b_ctx* gpu = nullptr;
+    std::unique_ptr<GpuSurrogate> gpu_sur;
     bool has_surrogate = false;
     ta3t_surrogate sur{};
     Xoshiro generator{0};
@@ -182,6 +205,8 @@ struct ta3t_trainer {
         return 0;
     }
 
+    ta3t_surrogate sur_builtin{};
+
     int init(ta3t_config const* c, ta3t_score_fn fn, void* u, ta3t_surrogate const* s, std::string const* state) {
         cfg = *c;
         if (cfg.islands == 0 || cfg.population < 5 || cfg.games == 0 || cfg.num_params == 0 ||
@@ -189,6 +214,16 @@ struct ta3t_trainer {
             return fail("ta3t_create: islands, games, num_params, gens and iterations must be positive, population >= 5");
         if (!(cfg.sigma0 > 0.0) || !(cfg.upper > cfg.lower)) return fail("ta3t_create: bad sigma0 or bounds");
         if (cfg.algo != TA3C_SEP && cfg.algo != TA3C_DD) return fail("ta3t_create: algo must be TA3C_SEP or TA3C_DD");
+        if (cfg.surrogate_start_gen && !s) {
+            gpu_sur = std::make_unique<GpuSurrogate>();
+            gpu_sur->model = ta3s_create(c->device, uint32_t(cfg.training_seed));
+            if (!gpu_sur->model) return fail(std::string("surrogate: ") + ta3s_last_error(nullptr));
+            if (cfg.surrogate_epochs) gpu_sur->epochs = cfg.surrogate_epochs;
+            if (cfg.surrogate_batch) gpu_sur->batch = cfg.surrogate_batch;
+            if (cfg.surrogate_lr > 0) gpu_sur->lr = float(cfg.surrogate_lr);
+            sur_builtin = ta3t_surrogate{gpu_sur.get(), gpu_sur_train, gpu_sur_predict};
+            s = &sur_builtin;
+        }
         if (cfg.surrogate_start_gen) {
             if (!s || !s->train || !s->predict) return fail("ta3t_create: pre-screening needs a surrogate");
             if (cfg.surrogate_top + cfg.surrogate_random < 5 ||
@@ -461,6 +496,9 @@ void ta3t_default_config(ta3t_config* c) {
     c->surrogate_random = 5;
     c->surrogate_retrain = 10;
     c->surrogate_min_rho = 0.6;
+    c->surrogate_epochs = 40;
+    c->surrogate_batch = 256;
+    c->surrogate_lr = 1e-3;
 }
 
 static ta3t_trainer* create(const ta3t_config* cfg, std::string const* state, ta3t_score_fn fn, void* user,

@@ -1,0 +1,105 @@
+"""Python binding of the GPU surrogate model (include/ta3b_surrogate.h, in
+libta3b.so): an MLP 97 -> 128 -> 128 -> 2 trained on (parameter vector ->
+mean score) pairs with hand-written tcgen05 forward / backward / Adam kernels.
+`train(x, y)` / `predict(x)` make it usable as the island trainer's surrogate."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from .evaluator import EvaluatorError, library
+
+_SIG = {
+    "ta3s_num_params": (C.c_uint32, []),
+    "ta3s_create": (C.c_void_p, [C.c_int, C.c_uint32]),
+    "ta3s_destroy": (None, [C.c_void_p]),
+    "ta3s_last_error": (C.c_char_p, [C.c_void_p]),
+    "ta3s_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ta3s_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ta3s_set_data": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "ta3s_set_data_standardized": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "ta3s_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ta3s_train": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.c_void_p]),
+    "ta3s_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+}
+SURROGATE_EXPORTS = sorted(_SIG)
+
+
+def _lib():
+    lib = library()
+    for name, (res, args) in _SIG.items():
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    return lib
+
+
+def _p(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+class Surrogate:
+    """The GPU surrogate. Raises EvaluatorError without an sm_100 device."""
+
+    def __init__(self, device: int = 0, seed: int = 0, epochs: int = 40, batch: int = 256, lr: float = 1e-3,
+                 weight_decay: float = 1e-2):
+        self.lib = _lib()
+        self.h = self.lib.ta3s_create(device, seed)
+        if not self.h:
+            raise EvaluatorError(self.lib.ta3s_last_error(None).decode())
+        self.nparam = int(self.lib.ta3s_num_params())
+        self.epochs, self.batch, self.lr, self.wd, self.seed = epochs, batch, lr, weight_decay, seed
+        self.trainings = 0
+        self.last_loss = float("nan")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.lib.ta3s_destroy(self.h)
+            self.h = None
+
+    def _ok(self, rc):
+        if rc:
+            raise EvaluatorError(self.lib.ta3s_last_error(self.h).decode())
+
+    @property
+    def params(self) -> np.ndarray:
+        out = np.empty(self.nparam, np.float32)
+        self._ok(self.lib.ta3s_get_params(self.h, _p(out)))
+        return out
+
+    @params.setter
+    def params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == self.nparam
+        self._ok(self.lib.ta3s_set_params(self.h, _p(p)))
+
+    def gradients(self, x, y, standardized: bool = True):
+        """Gradient of the mean loss over (x, y) and the summed loss, no update."""
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        fn = self.lib.ta3s_set_data_standardized if standardized else self.lib.ta3s_set_data
+        self._ok(fn(self.h, _p(x), _p(y), len(y)))
+        g = np.empty(self.nparam, np.float32)
+        loss = C.c_float()
+        self._ok(self.lib.ta3s_gradients(self.h, _p(g), C.byref(loss)))
+        return g, loss.value
+
+    def train(self, x, y, epochs: int | None = None, batch: int | None = None, standardized: bool = False):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        fn = self.lib.ta3s_set_data_standardized if standardized else self.lib.ta3s_set_data
+        self._ok(fn(self.h, _p(x), _p(y), len(y)))
+        loss = C.c_float()
+        self._ok(self.lib.ta3s_train(self.h, epochs or self.epochs, batch or self.batch, self.lr, self.wd,
+                                     self.seed + self.trainings, C.byref(loss)))
+        self.trainings += 1
+        self.last_loss = loss.value
+        return loss.value
+
+    def predict(self, x, with_logvar: bool = False):
+        x = np.ascontiguousarray(x, np.float32)
+        n = len(x)
+        mean = np.empty(n, np.float32)
+        lv = np.empty(n, np.float32) if with_logvar else None
+        self._ok(self.lib.ta3s_predict(self.h, _p(x), n, _p(mean), _p(lv)))
+        return (mean, lv) if with_logvar else mean

@@ -35,7 +35,8 @@ class TrainerConfig(C.Structure):
                 ("sigma0", C.c_double), ("lower", C.c_double), ("upper", C.c_double), ("device", C.c_int),
                 ("surrogate_start_gen", C.c_uint32), ("surrogate_sample", C.c_uint32),
                 ("surrogate_top", C.c_uint32), ("surrogate_random", C.c_uint32),
-                ("surrogate_retrain", C.c_uint32), ("surrogate_min_rho", C.c_double)]
+                ("surrogate_retrain", C.c_uint32), ("surrogate_min_rho", C.c_double),
+                ("surrogate_epochs", C.c_uint32), ("surrogate_batch", C.c_uint32), ("surrogate_lr", C.c_double)]
 
 
 class TrainerStats(C.Structure):
