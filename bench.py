@@ -45,6 +45,11 @@ UNIT = "placements/s"
 # (16 + 46 per column x 10 + 11); MLP 8 x (10 mul + 10 add + relu) + 8 mul + 8 add
 # (192); key (6) = 1010.
 REF_OPS_PER_PLACEMENT = 1010
+# The widened 10 -> 64 -> 64 -> 1 network replaces the MLP's 192 by
+# 64 x (10 mul + 10 add + relu) + 64 x (64 mul + 64 add + relu) + 64 mul + 64 add = 9,728.
+REF_OPS_PER_PLACEMENT_WIDE = 1010 - 192 + 9728
+METRIC_WIDE = ("beam placements/s on 1 B200 (widened 10-64-64-1 evaluator: 8 islands x 100 models x 100 games "
+               "= 80k sims, cap 2000)")
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
 # on the small-case capture) and its DRAM bytes per full-generation launch
 # (ncu dram__bytes_read.sum + dram__bytes_write.sum, captured at 200 and 800 sims:
@@ -114,23 +119,27 @@ class ClockSampler:
                 if any(r[3].replace('.', '').isdigit() for r in rows) else None}
 
 
-def _ref_lib():
-    """The reference's CPU path (oracle/_ref) if built, else the oracle's restatement."""
+def _ref_lib(wide: bool = False):
+    """The reference's CPU path (oracle/_ref) if built, else the oracle's restatement,
+    as (batch function with the ta3ref_eval_mt signature, kind)."""
     ref = os.path.join(ROOT, "oracle", "_ref", "libta3ref.so")
     if os.path.exists(ref):
-        return C.CDLL(ref), "ta3ref_eval_mt", "reference"
+        lib = C.CDLL(ref)
+        return (lib.ta3ref_eval_wide_mt if wide else lib.ta3ref_eval_mt), "reference"
     port = os.path.join(ROOT, "oracle", "_build", "libta3oracle.so")
     if not os.path.exists(port):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
-    return C.CDLL(port), "ta3o_eval_mt", "port"
+    lib = C.CDLL(port)
+    if wide:
+        return (lambda *a: lib.ta3o_eval_net_mt(a[0], 64, 64, *a[1:])), "port"
+    return lib.ta3o_eval_mt, "port"
 
 
 def cpu_rate(batch: workload.Batch, budget_s: float, threads: int):
     """Placements/s of the CPU path over a bounded sample of the batch: whole
     models of island 0 (each with its island's games), in workload order,
     `threads` host threads over the (model, game) pairs, until budget_s."""
-    lib, fn, kind = _ref_lib()
-    f = getattr(lib, fn)
+    f, kind = _ref_lib(batch.weights.shape[1] == workload.NUM_PARAMS_WIDE)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
     games = batch.games
     mpi = batch.models // batch.islands
@@ -143,7 +152,8 @@ def cpu_rate(batch: workload.Batch, budget_s: float, threads: int):
         sc = np.zeros(c * games, np.float32)
         evs = C.c_uint64()
         t0 = time.perf_counter()
-        f(p(w), c, p(seeds), games, batch.max_moves, threads, p(sc), None, None, C.byref(evs))
+        f(p(w), C.c_uint32(c), p(seeds), C.c_uint32(games), C.c_uint32(batch.max_moves), C.c_uint32(threads), p(sc),
+          None, None, C.byref(evs))
         t_used += time.perf_counter() - t0
         total_ev += evs.value
         models += c
@@ -157,11 +167,21 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def _batch(args, rank: int = 0) -> workload.Batch:
+    """The workload of one rank (weak scaling: rank r scores generation seed base+r)."""
+    if args.model == "wide":
+        return workload.wide_batch(islands=args.islands or 8, pop=args.pop or 100, games=args.games or 100,
+                                   max_moves=args.cap or 2000, seed=rank_seed(3, rank))
+    return workload.generation_batch(islands=args.islands or 4, pop=args.pop or 50, games=args.games or 50,
+                                     max_moves=args.cap or 2000, seed=rank_seed(1, rank))
+
+
 def run_reference(args):
     rank, world, _ = _dist_env()
     if rank != 0:
         return
-    batch = workload.generation_batch()
+    batch = _batch(args)
+    metric = METRIC_WIDE if args.model == "wide" else METRIC
     threads = host_threads()
     rates = []
     kind = "reference"
@@ -170,9 +190,10 @@ def run_reference(args):
         r, kind, sims, t = cpu_rate(batch, budget_s=args.ref_budget, threads=threads)
         if step >= args.warmup:
             rates.append(r)
-            sample_desc = f"first {sims} sims of the generation (island 0, model-major), cap 2000, {t:.1f} s per step"
+            sample_desc = (f"first {sims} sims of the generation (island 0, model-major), cap {batch.max_moves}, "
+                           f"{t:.1f} s per step")
     v = float(np.mean(rates))
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    line = {"impl": "reference", "metric": metric, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "fp32+int32", "data": "synthetic",
             "config": {"workload": batch.name, "global_batch": batch.sims, "seq_len": batch.max_moves,
@@ -204,8 +225,10 @@ def run_ours(args):
     if world > 1:
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     # weak scaling: each rank scores its own generation (islands seeded per rank)
-    batch = workload.generation_batch(islands=args.islands, pop=args.pop, games=args.games, max_moves=args.cap,
-                             seed=rank_seed(1, rank))
+    batch = _batch(args, rank)
+    wide = args.model == "wide"
+    metric = METRIC_WIDE if wide else METRIC
+    ops_per_placement = REF_OPS_PER_PLACEMENT_WIDE if wide else REF_OPS_PER_PLACEMENT
     ev = ModelEvaluator(device=local)
     stream = torch.cuda.Stream(device=dev)
     w_dev = torch.from_numpy(batch.weights).to(dev)
@@ -225,7 +248,7 @@ def run_ours(args):
     tune = None
     if args.variant >= 0:
         ev.select_variant(args.variant)
-    elif not args.no_autotune:
+    elif not args.no_autotune and not wide:
         tune = ev.autotune(w_dev, s_dev, batch.max_moves, score, pieces, lines, evals, batch.islands, stream)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -268,7 +291,8 @@ def run_ours(args):
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        rc = lib.ta3b_eval_islands(ev._ctx, vp(h_w), batch.islands, batch.models // batch.islands, 97, vp(h_s),
+        rc = lib.ta3b_eval_islands(ev._ctx, vp(h_w), batch.islands, batch.models // batch.islands,
+                                   batch.weights.shape[1], vp(h_s),
                                    batch.games, batch.max_moves, vp(h_sc), vp(h_pc), vp(h_lc))
         if rc:
             raise RuntimeError(lib.ta3b_last_error(ev._ctx).decode())
@@ -284,22 +308,25 @@ def run_ours(args):
         sm_mhz = float(peaks.get("sm_max_mhz", 1965.0))
         peak_issue = sms * 4 * 32 * sm_mhz * 1e6 / 1e12            # lane-instructions, T/s
         per_gpu = value / world
-        ach = per_gpu * REF_OPS_PER_PLACEMENT / 1e12
+        ach = per_gpu * ops_per_placement / 1e12
         roof = {"bound": "issue", "achieved": ach, "peak": peak_issue, "unit": "T int32/fp32 lane-ops/s",
                 "frac": ach / peak_issue, "traffic": DRAM_BYTES_PER_LAUNCH,
                 "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz {sm_mhz:.0f} "
                                f"(MEASURED_PEAKS.json, {kind})",
-                "ops_per_placement": REF_OPS_PER_PLACEMENT,
+                "ops_per_placement": ops_per_placement,
                 "ops_basis": "reference algorithm per-placement operation count (hand count above)",
-                "lane_instr_per_placement_measured": LANE_INSTR_PER_PLACEMENT,
-                "issue_frac_measured": per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12 / peak_issue}
+                "lane_instr_per_placement_measured": None if wide else LANE_INSTR_PER_PLACEMENT,
+                "issue_frac_measured": None if wide else per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12 / peak_issue}
+        if wide:
+            roof["traffic"] = None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             threads = host_threads()
             r, ck, sims, t = cpu_rate(batch, budget_s=args.cpu_budget, threads=threads)
             cpu = {"value": r, "unit": UNIT, "cores": threads, "kind": ck,
-                   "sample": f"first {sims} sims of the generation (island 0, model-major), cap 2000, {t:.1f} s"}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                   "sample": f"first {sims} sims of the generation (island 0, model-major), cap {batch.max_moves}, "
+                             f"{t:.1f} s"}
+        line = {"metric": metric, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "fp32+int32", "data": "synthetic",
                 "config": {"workload": batch.name, "global_batch": batch.sims * world, "seq_len": batch.max_moves,
@@ -329,11 +356,13 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="fixed kernel variant (default: autotune)")
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--model", choices=["v11", "wide"], default="v11",
+                    help="v11 (headline) or the widened 10-64-64-1 evaluator's 80k-sim generation")
     # reduced shapes for profiling captures only (the headline is the default full generation)
-    ap.add_argument("--islands", type=int, default=4)
-    ap.add_argument("--pop", type=int, default=50)
-    ap.add_argument("--games", type=int, default=50)
-    ap.add_argument("--cap", type=int, default=2000)
+    ap.add_argument("--islands", type=int, default=0)
+    ap.add_argument("--pop", type=int, default=0)
+    ap.add_argument("--games", type=int, default=0)
+    ap.add_argument("--cap", type=int, default=0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

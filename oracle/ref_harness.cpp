@@ -49,12 +49,50 @@ struct game_out {
     std::uint64_t evals;
 };
 
+// The reference's customizable architecture widened: the v11 inputs
+// (ModelV11::extractInputs, model_v11.hpp:63-91) through the reference's own
+// dense layers (utility.hpp:29-46) 10 -> 64 ReLU -> 64 ReLU -> 1, weights of
+// each layer as [out][in] then [out] biases: 704 + 4160 + 65 = 4,929 parameters.
+constexpr std::size_t WIDE_H = 64;
+constexpr std::size_t WIDE_L1 = 10 * WIDE_H + WIDE_H, WIDE_L2 = WIDE_H * WIDE_H + WIDE_H, WIDE_L3 = WIDE_H + 1;
+constexpr std::size_t WIDE_P = WIDE_L1 + WIDE_L2 + WIDE_L3;
+
+struct counting_wide {
+    float const* w;
+    std::uint64_t* counter;
+    [[nodiscard]] search::value_t evaluate(search::clear_t c, sim::Board2 const& b, bool held_i) const {
+        ++*counter;
+        std::array<ai::data_t, ai::ModelV11::INPUTS> in{};
+        ai::ModelV11::extractInputs(c, b, held_i, in);
+        auto const h1 = ai::dense<10, WIDE_H, true>(in, std::span<ai::data_t const, WIDE_L1>{w, WIDE_L1});
+        auto const h2 = ai::dense<WIDE_H, WIDE_H, true>(h1, std::span<ai::data_t const, WIDE_L2>{w + WIDE_L1, WIDE_L2});
+        return ai::dense<WIDE_H, 1, false>(h2, std::span<ai::data_t const, WIDE_L3>{w + WIDE_L1 + WIDE_L2, WIDE_L3})[0];
+    }
+};
+
 // The loop of ModelEvaluator::eval_host (model_eval_host.cpp:35-51), with the
 // piece / line counts and an optional per-move trace recorded on the side.
+template<class Model>
+game_out play_with(Model const& model, std::uint64_t& evals, std::uint64_t seed, std::uint32_t max_moves,
+                   std::uint8_t* trace, std::uint32_t* n_moves, std::uint32_t* board_out);
+
 game_out play(float const* w, std::uint64_t seed, std::uint32_t max_moves, std::uint8_t* trace,
               std::uint32_t* n_moves, std::uint32_t* board_out) {
     std::uint64_t evals = 0;
     counting_ref const model{ta3::gpu::net_ref{ai::model_t::weights_t{w, P}}, &evals};
+    return play_with(model, evals, seed, max_moves, trace, n_moves, board_out);
+}
+
+game_out play_wide(float const* w, std::uint64_t seed, std::uint32_t max_moves, std::uint8_t* trace,
+                   std::uint32_t* n_moves, std::uint32_t* board_out) {
+    std::uint64_t evals = 0;
+    counting_wide const model{w, &evals};
+    return play_with(model, evals, seed, max_moves, trace, n_moves, board_out);
+}
+
+template<class Model>
+game_out play_with(Model const& model, std::uint64_t& evals, std::uint64_t seed, std::uint32_t max_moves,
+                   std::uint8_t* trace, std::uint32_t* n_moves, std::uint32_t* board_out) {
     sim::TetrisEngine game{seed};
     ai::stats_v4 stats{};
     std::uint32_t lines = 0, moves = 0;
@@ -90,6 +128,19 @@ game_out play(float const* w, std::uint64_t seed, std::uint32_t max_moves, std::
 extern "C" {
 
 std::uint32_t ta3ref_num_params() { return static_cast<std::uint32_t>(P); }
+std::uint32_t ta3ref_num_params_wide() { return static_cast<std::uint32_t>(WIDE_P); }
+
+// One game of the widened 10 -> 64 -> 64 -> 1 model, with its trace.
+int ta3ref_play_wide(float const* w, std::uint64_t seed, std::uint32_t max_moves, float* score, std::uint32_t* pieces,
+                     std::uint32_t* lines, std::uint64_t* evals, std::uint8_t* trace, std::uint32_t* n_moves,
+                     std::uint32_t* board_out) {
+    auto const r = play_wide(w, seed, max_moves, trace, n_moves, board_out);
+    *score = r.score;
+    *pieces = r.pieces;
+    *lines = r.lines;
+    *evals = r.evals;
+    return 0;
+}
 
 // ModelEvaluator::eval_host itself, once per model (model-major output).
 int ta3ref_eval_host(float const* w, std::uint32_t num_models, std::uint64_t const* seeds, std::uint32_t num_games,
@@ -118,9 +169,15 @@ int ta3ref_play(float const* w, std::uint64_t seed, std::uint32_t max_moves, flo
 
 // Multi-threaded batch over (model, game) pairs, pulled from an atomic ticket;
 // the CPU baseline. Returns wall-clock-free results; the caller times it.
-int ta3ref_eval_mt(float const* w, std::uint32_t num_models, std::uint64_t const* seeds, std::uint32_t num_games,
-                   std::uint32_t max_moves, std::uint32_t threads, float* score_out, std::uint32_t* pieces_out,
-                   std::uint32_t* lines_out, std::uint64_t* evals_total) {
+} // extern "C"
+
+namespace {
+using play_fn = game_out (*)(float const*, std::uint64_t, std::uint32_t, std::uint8_t*, std::uint32_t*,
+                             std::uint32_t*);
+
+int eval_mt(play_fn fn, std::size_t stride, float const* w, std::uint32_t num_models, std::uint64_t const* seeds,
+            std::uint32_t num_games, std::uint32_t max_moves, std::uint32_t threads, float* score_out,
+            std::uint32_t* pieces_out, std::uint32_t* lines_out, std::uint64_t* evals_total) {
     std::uint64_t const total = static_cast<std::uint64_t>(num_models) * num_games;
     std::atomic<std::uint64_t> next{0};
     std::atomic<std::uint64_t> evals{0};
@@ -131,7 +188,7 @@ int ta3ref_eval_mt(float const* w, std::uint32_t num_models, std::uint64_t const
             if(i >= total)
                 break;
             auto const m = i / num_games, g = i % num_games;
-            auto const r = play(w + m * P, seeds[g], max_moves, nullptr, nullptr, nullptr);
+            auto const r = fn(w + m * stride, seeds[g], max_moves, nullptr, nullptr, nullptr);
             score_out[i] = r.score;
             if(pieces_out)
                 pieces_out[i] = r.pieces;
@@ -153,6 +210,24 @@ int ta3ref_eval_mt(float const* w, std::uint32_t num_models, std::uint64_t const
     if(evals_total)
         *evals_total = evals.load();
     return 0;
+}
+} // namespace
+
+extern "C" {
+
+int ta3ref_eval_mt(float const* w, std::uint32_t num_models, std::uint64_t const* seeds, std::uint32_t num_games,
+                   std::uint32_t max_moves, std::uint32_t threads, float* score_out, std::uint32_t* pieces_out,
+                   std::uint32_t* lines_out, std::uint64_t* evals_total) {
+    return eval_mt(play, P, w, num_models, seeds, num_games, max_moves, threads, score_out, pieces_out, lines_out,
+                   evals_total);
+}
+
+// the same batch for the widened 10 -> 64 -> 64 -> 1 model (4,929 parameters per model)
+int ta3ref_eval_wide_mt(float const* w, std::uint32_t num_models, std::uint64_t const* seeds, std::uint32_t num_games,
+                        std::uint32_t max_moves, std::uint32_t threads, float* score_out, std::uint32_t* pieces_out,
+                        std::uint32_t* lines_out, std::uint64_t* evals_total) {
+    return eval_mt(play_wide, WIDE_P, w, num_models, seeds, num_games, max_moves, threads, score_out, pieces_out,
+                   lines_out, evals_total);
 }
 
 // Weights of ta3_gpu/tests/src/parity_test.cpp:20-32: mt19937{seed} with

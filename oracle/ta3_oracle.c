@@ -391,24 +391,43 @@ static void extract_inputs(uint32_t clear_bits, board_t const* b, int held_is_i,
     in[9] = (float)m.wells / 5.0f;
 }
 
-/* model_v11.hpp:166-180 + utility.hpp:30-46: 10 -> 8 ReLU -> 1, bias first, inputs ascending */
-static float forward(float const in[NIN], float const* w) {
-    float hdn[NHID];
-    for (int o = 0; o < NHID; ++o) {
-        float v = w[NIN * NHID + o];
-        for (int i = 0; i < NIN; ++i) v += in[i] * w[o * NIN + i];
-        hdn[o] = (0.0f < v) ? v : 0.0f;               /* std::max<float>(0, v) */
-    }
-    float const* w2 = w + NIN * NHID + NHID;
-    float v = w2[NHID];
-    for (int i = 0; i < NHID; ++i) v += hdn[i] * w2[i];
-    return v;
+/* The value network: the v11 inputs through dense layers (utility.hpp:29-46:
+ * per output unit, bias first, then inputs ascending; weights [out][in] then
+ * [out] biases per layer). v11 (model_v11.hpp:166-180) is h1 = 8, h2 = 0:
+ * 10 -> 8 ReLU -> 1. The widened architecture is h1 = h2 = 64:
+ * 10 -> 64 ReLU -> 64 ReLU -> 1. */
+#define MAXH 64
+typedef struct { float const* w; uint32_t h1, h2; } net_t;
+
+static uint32_t net_params(uint32_t h1, uint32_t h2) {
+    return h2 ? NIN * h1 + h1 + h1 * h2 + h2 + h2 + 1 : NIN * h1 + h1 + h1 + 1;
 }
 
-static float evaluate(uint32_t clear_bits, board_t const* b, int held_is_i, float const* w) {
+static void dense(float const* in, uint32_t n_in, float const* w, uint32_t n_out, int relu, float* out) {
+    for (uint32_t o = 0; o < n_out; ++o) {
+        float v = w[n_in * n_out + o];
+        for (uint32_t i = 0; i < n_in; ++i) v += in[i] * w[o * n_in + i];
+        out[o] = relu ? ((0.0f < v) ? v : 0.0f) : v;  /* std::max<float>(0, v) */
+    }
+}
+
+static float forward(float const in[NIN], net_t const* net) {
+    float h1[MAXH], h2[MAXH], out;
+    dense(in, NIN, net->w, net->h1, 1, h1);
+    float const* w2 = net->w + NIN * net->h1 + net->h1;
+    if (!net->h2) {
+        dense(h1, net->h1, w2, 1, 0, &out);
+        return out;
+    }
+    dense(h1, net->h1, w2, net->h2, 1, h2);
+    dense(h2, net->h2, w2 + net->h1 * net->h2 + net->h2, 1, 0, &out);
+    return out;
+}
+
+static float evaluate(uint32_t clear_bits, board_t const* b, int held_is_i, net_t const* net) {
     float in[NIN];
     extract_inputs(clear_bits, b, held_is_i, in);
-    return forward(in, w);
+    return forward(in, net);
 }
 
 /* ------------------------------------------------- beam.hpp search --- */
@@ -447,7 +466,7 @@ typedef struct { int orient, x, hold; float value; int none; } result_t;
 static uint32_t clear_bump(int cleared) { return cleared == 0 ? 0u : 1u << (8 * (cleared - 1)); }  /* model_defs.hpp:37-43 */
 
 /* beam.hpp:484-570 (search_move_beam) with the stages of beam.hpp:283-470 */
-static result_t search_move_beam(engine_t const* g, float const* w, uint64_t* evals) {
+static result_t search_move_beam(engine_t const* g, net_t const* w, uint64_t* evals) {
     result_t res = {0, 0, 0, -INFINITY, 1};
     if (g->over) return res;
     enum { ROOT_SLOTS = 2 * MP, MID_SLOTS = 32 * 2 * MP, LEAF_ORDERS = 32 * 2 * MP, SPAN = LEAF_ORDERS + 16 };
@@ -601,8 +620,8 @@ static double score_v1(stats_t const* s) {                /* score_v1.hpp:8-34 *
 
 /* ------------------------------------------------------- C ABI ------ */
 /* model_eval_host.cpp:35-51: one game, optional per-move trace (hold, orientation, x+2) */
-int ta3o_play(float const* w, uint64_t seed, uint32_t max_moves, float* score, uint32_t* pieces, uint32_t* lines,
-              uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint32_t* board_out) {
+static int play_net(net_t const* w, uint64_t seed, uint32_t max_moves, float* score, uint32_t* pieces,
+                    uint32_t* lines, uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint32_t* board_out) {
     ensure_ready();
     engine_t g; engine_reset(&g, seed);
     stats_t st; memset(&st, 0, sizeof st);
@@ -625,6 +644,23 @@ int ta3o_play(float const* w, uint64_t seed, uint32_t max_moves, float* score, u
     return 0;
 }
 
+int ta3o_play(float const* w, uint64_t seed, uint32_t max_moves, float* score, uint32_t* pieces, uint32_t* lines,
+              uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint32_t* board_out) {
+    net_t const net = {w, NHID, 0};
+    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, board_out);
+}
+
+/* one game of a dense value network with hidden widths h1, h2 (h2 = 0: one hidden layer) */
+int ta3o_play_net(float const* w, uint32_t h1, uint32_t h2, uint64_t seed, uint32_t max_moves, float* score,
+                  uint32_t* pieces, uint32_t* lines, uint64_t* evals, uint8_t* trace, uint32_t* n_moves,
+                  uint32_t* board_out) {
+    if (h1 == 0 || h1 > MAXH || h2 > MAXH) return 1;
+    net_t const net = {w, h1, h2};
+    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, board_out);
+}
+
+uint32_t ta3o_net_params(uint32_t h1, uint32_t h2) { return net_params(h1, h2); }
+
 /* ModelEvaluator::eval_host semantics batched over models, model-major outputs */
 int ta3o_eval(float const* w, uint32_t num_models, uint64_t const* seeds, uint32_t num_games, uint32_t max_moves,
               float* score_out, uint32_t* pieces_out, uint32_t* lines_out, uint64_t* evals_total) {
@@ -644,7 +680,7 @@ int ta3o_eval(float const* w, uint32_t num_models, uint64_t const* seeds, uint32
 }
 
 typedef struct {
-    float const* w; uint64_t const* seeds; uint32_t num_models, num_games, max_moves;
+    float const* w; uint32_t h1, h2; uint64_t const* seeds; uint32_t num_models, num_games, max_moves;
     float* score; uint32_t* pieces; uint32_t* lines;
     uint64_t next, evals; pthread_mutex_t mu;
 } mt_job_t;
@@ -659,7 +695,8 @@ static void* mt_worker(void* arg) {
         pthread_mutex_unlock(&j->mu);
         if (i >= total) break;
         uint64_t e = 0; float s; uint32_t p, l;
-        ta3o_play(j->w + (i / j->num_games) * NPARAMS, j->seeds[i % j->num_games], j->max_moves, &s, &p, &l, &e, 0, 0, 0);
+        net_t const net = {j->w + (i / j->num_games) * net_params(j->h1, j->h2), j->h1, j->h2};
+        play_net(&net, j->seeds[i % j->num_games], j->max_moves, &s, &p, &l, &e, 0, 0, 0);
         j->score[i] = s;
         if (j->pieces) j->pieces[i] = p;
         if (j->lines) j->lines[i] = l;
@@ -672,10 +709,12 @@ static void* mt_worker(void* arg) {
 }
 
 /* the same batch spread over `threads` host threads, (model, game) pairs pulled from a shared ticket */
-int ta3o_eval_mt(float const* w, uint32_t num_models, uint64_t const* seeds, uint32_t num_games, uint32_t max_moves,
-                 uint32_t threads, float* score_out, uint32_t* pieces_out, uint32_t* lines_out, uint64_t* evals_total) {
+static int eval_net_mt(float const* w, uint32_t h1, uint32_t h2, uint32_t num_models, uint64_t const* seeds,
+                       uint32_t num_games, uint32_t max_moves, uint32_t threads, float* score_out,
+                       uint32_t* pieces_out, uint32_t* lines_out, uint64_t* evals_total) {
     ensure_ready();
-    mt_job_t j = {w, seeds, num_models, num_games, max_moves, score_out, pieces_out, lines_out, 0, 0, PTHREAD_MUTEX_INITIALIZER};
+    mt_job_t j = {w, h1, h2, seeds, num_models, num_games, max_moves, score_out, pieces_out, lines_out, 0, 0,
+                  PTHREAD_MUTEX_INITIALIZER};
     if (threads < 1) threads = 1;
     if (threads > 256) threads = 256;
     pthread_t th[256];
@@ -683,6 +722,21 @@ int ta3o_eval_mt(float const* w, uint32_t num_models, uint64_t const* seeds, uin
     for (uint32_t t = 0; t < threads; ++t) pthread_join(th[t], 0);
     if (evals_total) *evals_total = j.evals;
     return 0;
+}
+
+int ta3o_eval_mt(float const* w, uint32_t num_models, uint64_t const* seeds, uint32_t num_games, uint32_t max_moves,
+                 uint32_t threads, float* score_out, uint32_t* pieces_out, uint32_t* lines_out, uint64_t* evals_total) {
+    return eval_net_mt(w, NHID, 0, num_models, seeds, num_games, max_moves, threads, score_out, pieces_out, lines_out,
+                       evals_total);
+}
+
+/* the batch for a dense network with hidden widths h1, h2 */
+int ta3o_eval_net_mt(float const* w, uint32_t h1, uint32_t h2, uint32_t num_models, uint64_t const* seeds,
+                     uint32_t num_games, uint32_t max_moves, uint32_t threads, float* score_out, uint32_t* pieces_out,
+                     uint32_t* lines_out, uint64_t* evals_total) {
+    if (h1 == 0 || h1 > MAXH || h2 > MAXH) return 1;
+    return eval_net_mt(w, h1, h2, num_models, seeds, num_games, max_moves, threads, score_out, pieces_out, lines_out,
+                       evals_total);
 }
 
 uint32_t ta3o_placements(uint32_t piece, uint8_t* orient, int8_t* x, uint16_t* cols, int8_t* col0) {
@@ -729,7 +783,8 @@ float ta3o_evaluate(float const* w, uint32_t const* cols10, uint32_t clear_bits,
     ensure_ready();
     board_t b; memcpy(b.c, cols10, sizeof b.c);
     extract_inputs(clear_bits, &b, held_is_i, features10);
-    return forward(features10, w);
+    net_t const net = {w, NHID, 0};
+    return forward(features10, &net);
 }
 
 int ta3o_apply(uint32_t const* cols10, uint32_t piece, uint32_t index, uint32_t* out10, uint32_t* cleared) {

@@ -12,6 +12,8 @@ Outputs (committed; the tests read only these, never the reference):
   boards.json    board-primitive and value-model known answers on random boards
   games.json     whole games: score / pieces / lines / evaluated placements,
                  the per-move (hold, orientation, x) trace and the final board
+  wide.json      whole games of the widened 10 -> 64 -> 64 -> 1 network
+                 (``python tests/golden/gen_golden.py wide`` regenerates only it)
 """
 from __future__ import annotations
 
@@ -176,8 +178,38 @@ def games():
     return {"cases": cases}
 
 
+def play_wide(w, seed, cap):
+    s, p, l, e, nm = C.c_float(), C.c_uint32(), C.c_uint32(), C.c_uint64(), C.c_uint32()
+    tr = (C.c_uint8 * (3 * cap))()
+    bd = np.zeros(10, np.uint32)
+    REF.ta3ref_play_wide(ptr(w), C.c_uint64(seed), cap, C.byref(s), C.byref(p), C.byref(l), C.byref(e), tr,
+                         C.byref(nm), ptr(bd))
+    return {"seed": str(int(seed)), "max_moves": cap, "score": f32hex(s.value), "score_f": float(s.value),
+            "pieces": p.value, "lines": l.value, "evals": e.value, "moves": nm.value,
+            "trace": bytes(tr)[:3 * nm.value].hex(), "board": bd.tolist()}
+
+
+def wide():
+    """The widened 10 -> 64 -> 64 -> 1 network (the reference's dense layers,
+    ta3ref_play_wide): the first models of the widened generation workload
+    (N(0, 1/fan_in) from seed 3), its island-0 game seeds, cap 300. Weights are
+    stored as little-endian float32 in hex (4,929 per model)."""
+    assert REF.ta3ref_num_params_wide() == workload.NUM_PARAMS_WIDE
+    b = workload.wide_batch(islands=1, pop=6, games=3, max_moves=300)
+    cases = []
+    for m in range(b.models):
+        w = np.ascontiguousarray(b.weights[m])
+        res = [play_wide(w, int(sd), 300) for sd in b.seeds[0]]
+        cases.append({"model": m, "weights_hex": w.astype("<f4").tobytes().hex(), "results": res})
+        print("wide model", m, [r["pieces"] for r in res], flush=True)
+    return {"workload": b.name, "seeds": [str(int(x)) for x in b.seeds[0]], "max_moves": 300, "cases": cases}
+
+
 def main():
-    for name, fn in (("tables", tables), ("engine", engine), ("boards", boards), ("games", games)):
+    only = sys.argv[1:]
+    for name, fn in (("tables", tables), ("engine", engine), ("boards", boards), ("games", games), ("wide", wide)):
+        if only and name not in only:
+            continue
         data = fn()
         with open(os.path.join(HERE, f"{name}.json"), "w") as f:
             json.dump(data, f, separators=(",", ":"))

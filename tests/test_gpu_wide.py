@@ -1,0 +1,66 @@
+"""The widened network (10 -> 64 -> 64 -> 1, 4,929 weights per model) on the
+GPU kernel against the reference's own games (tests/golden/wide.json) and
+against the oracle on further random models: bit-exact scores, pieces, lines,
+evaluated placements and traces."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import f32_from_hex, load_golden, ptr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ev():
+    from tetris_ai3_b200 import ModelEvaluator
+    return ModelEvaluator(device=0)
+
+
+def _golden():
+    g = load_golden("wide")
+    w = np.stack([np.frombuffer(bytes.fromhex(c["weights_hex"]), "<f4") for c in g["cases"]]).astype(np.float32)
+    return g, w, np.array([int(s) for s in g["seeds"]], np.uint64)
+
+
+def test_wide_matches_reference_games(ev):
+    g, w, seeds = _golden()
+    out = ev.eval_trace(w, w.shape[0], seeds, g["max_moves"])
+    for m, case in enumerate(g["cases"]):
+        for k, r in enumerate(case["results"]):
+            i = m * seeds.size + k
+            assert out["score"][i] == f32_from_hex(r["score"]), (m, k)
+            assert out["pieces"][i] == r["pieces"] and out["lines"][i] == r["lines"], (m, k)
+            assert out["evals"][i] == r["evals"] and out["moves"][i] == r["moves"], (m, k)
+            assert bytes(out["trace"][i][:3 * r["moves"]]).hex() == r["trace"], (m, k)
+            assert out["board"][i].tolist() == r["board"], (m, k)
+
+
+def test_wide_random_models_match_oracle(ev, oracle):
+    from tetris_ai3_b200 import workload
+    b = workload.wide_batch(islands=2, pop=3, games=4, max_moves=150, seed=5)
+    sc, pc, lc = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    for isl in range(b.islands):
+        w = np.ascontiguousarray(b.weights[isl * 3:(isl + 1) * 3])
+        s = np.ascontiguousarray(b.seeds[isl])
+        n = w.shape[0] * s.size
+        osc, opc, olc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        ev_total = C.c_uint64()
+        oracle.ta3o_eval_net_mt(ptr(w), 64, 64, w.shape[0], ptr(s), s.size, b.max_moves, 8, ptr(osc), ptr(opc),
+                                ptr(olc), C.byref(ev_total))
+        lo, hi = isl * n, (isl + 1) * n
+        assert sc[lo:hi].tobytes() == osc.tobytes()
+        assert np.array_equal(pc[lo:hi], opc) and np.array_equal(lc[lo:hi], olc)
+
+
+def test_v11_and_wide_share_a_context(ev):
+    from tetris_ai3_b200 import workload
+    g, w, seeds = _golden()
+    a = ev.eval(w[:2], 2, seeds[:2], 60)
+    b1 = workload.single_model_batch()
+    v = ev.eval(b1.weights, 1, b1.seeds[0][:2], 60)
+    a2 = ev.eval(w[:2], 2, seeds[:2], 60)
+    assert a.tobytes() == a2.tobytes() and v.shape == (2,)

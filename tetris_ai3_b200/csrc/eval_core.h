@@ -222,6 +222,65 @@ TA3B_HD float value_full(uint32_t clear_bits, BoardInts const& bi, bool held_i, 
     return v;
 }
 
+// ---------------------------------------------- widened value network ---
+// The reference's dense layers (ta3_ai/incl/ta3/ai/models/models/utility.hpp:29-46)
+// widened: the v11 inputs -> 64 ReLU -> 64 ReLU -> 1, per layer [out][in]
+// weights then [out] biases (704 + 4160 + 65 = 4,929 parameters).
+constexpr int WH = 64;
+constexpr int WIDE_B1 = NIN * WH, WIDE_W2 = WIDE_B1 + WH, WIDE_B2 = WIDE_W2 + WH * WH, WIDE_W3 = WIDE_B2 + WH,
+              WIDE_B3 = WIDE_W3 + WH, NPARAMS_WIDE = WIDE_B3 + 1;
+static_assert(NPARAMS_WIDE == 4929, "10 -> 64 -> 64 -> 1");
+
+TA3B_HD float relu(float v) { return v > 0.0f ? v : 0.0f; }    // std::max<float>(0, v)
+
+// Every operation in the reference order (per output unit: bias, then inputs
+// ascending; layer 3 sums its inputs ascending). Layer 2's output units run four
+// at a time as independent chains, each still in reference order.
+template <class WF>
+TA3B_HD float wide_forward(float const (&in)[NIN], WF const& w) {
+    float h1[WH];
+#pragma unroll
+    for (int o = 0; o < WH; ++o) {
+        float v = w(WIDE_B1 + o);
+#pragma unroll
+        for (int i = 0; i < NIN; ++i) v = f_add(v, f_mul(in[i], w(o * NIN + i)));
+        h1[o] = relu(v);
+    }
+    float out = w(WIDE_B3);
+#pragma unroll 1
+    for (int o = 0; o < WH; o += 4) {
+        float a = w(WIDE_B2 + o), b = w(WIDE_B2 + o + 1), c = w(WIDE_B2 + o + 2), d = w(WIDE_B2 + o + 3);
+        int const r = WIDE_W2 + o * WH;
+#pragma unroll
+        for (int i = 0; i < WH; ++i) {
+            a = f_add(a, f_mul(h1[i], w(r + i)));
+            b = f_add(b, f_mul(h1[i], w(r + WH + i)));
+            c = f_add(c, f_mul(h1[i], w(r + 2 * WH + i)));
+            d = f_add(d, f_mul(h1[i], w(r + 3 * WH + i)));
+        }
+        out = f_add(out, f_mul(relu(a), w(WIDE_W3 + o)));
+        out = f_add(out, f_mul(relu(b), w(WIDE_W3 + o + 1)));
+        out = f_add(out, f_mul(relu(c), w(WIDE_W3 + o + 2)));
+        out = f_add(out, f_mul(relu(d), w(WIDE_W3 + o + 3)));
+    }
+    return out;
+}
+
+// model_v11.hpp:63-91 inputs, then the widened network
+template <class WF>
+TA3B_HD float value_full_wide(uint32_t clear_bits, BoardInts const& bi, bool held_i, WF const& w) {
+    float in[NIN];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) in[k] = f_mul(float((clear_bits >> (8 * k)) & 0xFFu), 0.25f);
+    in[4] = div_exact(bi.surf_sq > 0 ? f_sqrt(float(bi.surf_sq)) : 0.0f, 100.0f, R100);
+    in[5] = div_exact(float(bi.holes), 20.0f, R20);
+    in[6] = div_exact(float(bi.hole_depths), 200.0f, R200);
+    in[7] = float(bi.max_height);
+    in[8] = held_i ? 1.0f : 0.0f;
+    in[9] = div_exact(float(bi.wells), 5.0f, R5);
+    return wide_forward(in, w);
+}
+
 // --------------------------------------------------------- packed FP32x2 ---
 // Two independent, separately rounded FP32 operations per instruction on
 // sm_100 (__fmul2_rn / __fadd2_rn / __ffma2_rn: per component identical to the
@@ -425,7 +484,8 @@ TA3B_HD uint32_t partial_word(uint32_t clear_bits, int o, WF const& w) {
     return u;
 }
 
-template <class WF>
+// PARTIALS: the v11 hidden partial sums (the widened network recomputes its own per candidate)
+template <class WF, bool PARTIALS = true>
 TA3B_HD void build_record(uint32_t const (&b)[W], uint32_t clear_bits, WF const& w, uint32_t* rec) {
     ColumnData c;
     column_data(b, c);
@@ -445,8 +505,10 @@ TA3B_HD void build_record(uint32_t const (&b)[W], uint32_t clear_bits, WF const&
         combo_of(id, c0, wd);
         rec[R_COMBO + id] = combo_word(c, c0, wd);
     }
+    if (PARTIALS) {
 #pragma unroll
-    for (int o = 0; o < NHID; ++o) rec[R_P + o] = partial_word(clear_bits, o, w);
+        for (int o = 0; o < NHID; ++o) rec[R_P + o] = partial_word(clear_bits, o, w);
+    }
 }
 
 // ------------------------------------------------------------ fast path ---
@@ -489,9 +551,14 @@ struct RecView {
 // MLP_PTX_X2 = pairs of hidden units per packed PTX instruction (mul/add.rn.f32x2).
 enum MlpMode { MLP_SCALAR = 0, MLP_PTX_X2 = 1 };
 
-template <int MLP = MLP_SCALAR>
-TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& fw, float& value,
-                      float* dbg = nullptr) {
+// The fast path's features of one placement (holes, hole depths, surface,
+// wells, max height) from the parent record alone; true when the candidate
+// must take the full path instead.
+struct FastFeat {
+    int holes, hd, surf, wells, maxh, dr;
+};
+
+TA3B_HD bool fast_features(RecView const& r, PlaceFast pf, FastFeat& f) {
     int const width = int((pf.s >> 22) & 7u);
     // drop = min over the piece's columns of (top - lowest piece cell - 1), top = H - height
     int drop = 255, sumd = 0;
@@ -531,6 +598,16 @@ TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& 
     wells += int(rv && ((cb >> 21) & 1u) && nl >= hr + 3);
     int const hlw = lv ? hl : int(WALL), hrw = rv ? hr : int(WALL);
     wells += int(((pf.m >> 22) & 1u) && (hlw < hrw ? hlw : hrw) >= n0 + 3);
+    f = FastFeat{holes, hd, surf, wells, maxh, dr};
+    return defer;
+}
+
+template <int MLP = MLP_SCALAR>
+TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& fw, float& value,
+                      float* dbg = nullptr) {
+    FastFeat ff;
+    bool const defer = fast_features(r, pf, ff);
+    int const holes = ff.holes, hd = ff.hd, surf = ff.surf, wells = ff.wells, maxh = ff.maxh, dr = ff.dr;
     // features (model_v11.hpp:63-91): pairs of correctly rounded quotients
     float const sq = surf > 0 ? f_sqrt(float(surf)) : 0.0f;
     float2 const q56 = div2_exact(make_float2(float(holes), float(hd)), make_float2(20.0f, 200.0f),
@@ -581,6 +658,26 @@ TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& 
         v = f_add(v, t.y);
     }
     value = v;
+    return defer ? FAST_DEFER : FAST_OK;
+}
+
+// The fast path for the widened network: the same features, the parent's clear
+// counts as the first four inputs (a fast candidate clears no row).
+template <class WF>
+TA3B_HD int fast_eval_wide(RecView const& r, uint32_t clear_bits, PlaceFast pf, bool held_i, WF const& w,
+                           float& value) {
+    FastFeat ff;
+    bool const defer = fast_features(r, pf, ff);
+    float in[NIN];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) in[k] = f_mul(float((clear_bits >> (8 * k)) & 0xFFu), 0.25f);
+    in[4] = div_exact(ff.surf > 0 ? f_sqrt(float(ff.surf)) : 0.0f, 100.0f, R100);
+    in[5] = div_exact(float(ff.holes), 20.0f, R20);
+    in[6] = div_exact(float(ff.hd), 200.0f, R200);
+    in[7] = float(ff.maxh);
+    in[8] = held_i ? 1.0f : 0.0f;
+    in[9] = div_exact(float(ff.wells), 5.0f, R5);
+    value = defer ? 0.0f : wide_forward(in, w);
     return defer ? FAST_DEFER : FAST_OK;
 }
 

@@ -242,6 +242,21 @@ __device__ __forceinline__ int fast_candidate(uint32_t const* __restrict__ rec, 
     return fast_eval<MLP>(r, pf, held_i, fw, v, dbg);
 }
 
+// fast path of the widened network: the same record words, the weights from global memory
+__device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ rec, PlaceFast pf, bool held_i,
+                                                   float const* __restrict__ w, float& v) {
+    RecView r;
+    uint4 const q = *reinterpret_cast<uint4 const*>(rec + R_HD);
+    r.hd = q.x; r.rc0 = q.y; r.rc1 = q.z; r.rc2 = q.w;
+    r.tot = rec[R_TOT];
+    uint32_t const c0 = (pf.m >> 27) & 0xFu;
+    uint2 const sp = *reinterpret_cast<uint2 const*>(rec + R_SPAN + 2 * c0);
+    r.h4 = sp.x;
+    r.hm4 = sp.y;
+    r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
+    return fast_eval_wide(r, rec[R_CLEARS], pf, held_i, GlobalW{w}, v);
+}
+
 // stats_v4::advance (tetris_stats.hpp:19-23 with metrics.hpp:196-229)
 __device__ void stats_advance(Stats& st, uint32_t const* board, uint32_t lines) {
     uint32_t b[W];
@@ -310,7 +325,9 @@ __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
 // ---------------------------------------------------------------- kernel ---
 struct alignas(16) WarpShared {
     uint32_t rec[33][REC_WORDS];      // kept frontier records (rank -> record); [32] = committed board
-    float wfull[NPARAMS + 3];         // the model's weights (full path, record partial sums)
+    float wfull[NPARAMS + 3];         // the v11 model's weights (full path, record partial sums)
+    float const* wglobal;              // the widened model's weights (global memory)
+    uint32_t pad_[2];
     Engine eng;                        // the committed game
     Stats st;
     uint32_t seg_off[65];              // a level's candidate segments (parent rank, child list)
@@ -360,6 +377,7 @@ struct Luts {
 
 // Full path for one queued candidate (segment << 8 | placement): its key, or 0 if illegal.
 // A legal candidate's key is never 0 (its low word is a positive position).
+template <bool WIDE>
 __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, uint32_t entry) {
     uint32_t const seg = entry >> 8, i = entry & 0xFFu;
     uint32_t const info = ws->seg_info[seg];
@@ -370,7 +388,8 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
     int cl = 0;
     if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return 0;
     BoardInts const bi = board_ints(nb);
-    float const v = value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
+    float const v = WIDE ? value_full_wide(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, GlobalW{ws->wglobal})
+                         : value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
     return candidate_key(leaf, v, info, i);
 }
 
@@ -378,6 +397,7 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality.
+template <bool WIDE>
 __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, bool leaf, uint32_t total,
                                                int kl, int lane, uint32_t& evals) {
     LevelAcc acc{0, 0, 0, 0, 0};
@@ -397,7 +417,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
         uint64_t key = 0;
         if (uint32_t(lane) < n) {
             uint32_t const entry = ws.defer[lane];
-            key = full_key(&ws, lut, leaf, entry);
+            key = full_key<WIDE>(&ws, lut, leaf, entry);
             consume(key, entry >> 8, ws.seg_info[entry >> 8]);
         }
         fold(key);
@@ -431,9 +451,14 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
         float v[TA3B_ILP];
         int st[TA3B_ILP];
 #pragma unroll
-        for (int u = 0; u < TA3B_ILP; ++u)
-            st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]], (info[u] >> 20) & 1u,
-                                   fw, v[u]);
+        for (int u = 0; u < TA3B_ILP; ++u) {
+            if (WIDE)
+                st[u] = fast_candidate_wide(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
+                                            (info[u] >> 20) & 1u, ws.wglobal, v[u]);
+            else
+                st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
+                                       (info[u] >> 20) & 1u, fw, v[u]);
+        }
 #pragma unroll
         for (int u = 0; u < TA3B_ILP; ++u) {
             uint64_t key = 0;
@@ -495,6 +520,7 @@ __device__ __forceinline__ uint32_t build_segments(WarpShared& ws, uint32_t cons
 }
 
 // lane j builds kept node j (when active): parent record `prec`, placement (piece, i)
+template <bool WIDE>
 __device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, uint32_t prec, uint32_t piece,
                                          uint32_t i, int lane) {
     uint32_t nb[W];
@@ -509,21 +535,23 @@ __device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, 
         ncl = pr[R_CLEARS] + clear_bump(cl);
     }
     __syncwarp();
-    if (active) build_record(nb, ncl, SmemW{ws->wfull}, ws->rec[lane]);
+    if (active) build_record<SmemW, !WIDE>(nb, ncl, SmemW{ws->wfull}, ws->rec[lane]);
     __syncwarp();
 }
 
 // the committed board's record (record 32): one lane builds it, the warp waits
+template <bool WIDE>
 __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
     if (lane == 0) {
         uint32_t b[W];
         load_board(ws->eng.board, b);
-        build_record(b, 0u, SmemW{ws->wfull}, ws->rec[32]);
+        build_record<SmemW, !WIDE>(b, 0u, SmemW{ws->wfull}, ws->rec[32]);
     }
     __syncwarp();
 }
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
+template <bool WIDE>
 __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, int lane, uint32_t& evals,
                                             uint32_t* status) {
     Move mv{0, 0, 0, true};
@@ -546,7 +574,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         // ---- segments of this stage
         uint32_t total;
         if (stage == 0) {                      // two root groups over the committed board (beam.hpp:283-301)
-            root_record(&ws, lane);
+            root_record<WIDE>(&ws, lane);
             if (lane < 2) {
                 uint32_t const nd = lane ? r1 : r0;
                 uint32_t const held_slot = (nd >> 4) & 0xFu;
@@ -565,7 +593,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
         // ---- every candidate of the stage
-        LevelAcc const a = level_pass(ws, lut, fw, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane, evals);
+        LevelAcc const a = level_pass<WIDE>(ws, lut, fw, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane,
+                                            evals);
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
             kept = __popc(__ballot_sync(FULL_MASK, a.list != 0));
@@ -574,7 +603,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             fscore = uint32_t(a.list >> 32);
             uint32_t const g = lane < kept ? root_slot / MP : 0u;
             fnode = g;
-            materialize(&ws, lut, lane < kept, 32u, g ? p1 : p0, root_slot % MP, lane);
+            materialize<WIDE>(&ws, lut, lane < kept, 32u, g ? p1 : p0, root_slot % MP, lane);
         } else if (!leaf) {
             uint32_t const has_child = __reduce_or_sync(FULL_MASK, a.lo);
             // kept nodes with no legal continuation become leaves at this depth (beam.hpp:549-551)
@@ -591,7 +620,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             uint32_t const par_rank = __shfl_sync(FULL_MASK, frank, int(pk));
             uint32_t const cnode = (2u * par_node + child) & 15u;
             uint32_t const piece = slot_piece[c_tables.node[tree][stage][cnode] & 0xFu];
-            materialize(&ws, lut, lane < next, pk, piece, sslot % MP, lane);
+            materialize<WIDE>(&ws, lut, lane < next, pk, piece, sslot % MP, lane);
             fscore = uint32_t(a.list >> 32);
             fnode = lane < next ? cnode : 0u;
             frank = par_rank;
@@ -633,7 +662,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     return mv;
 }
 
-template <int WARPS, int MINB>
+// WIDE: the widened 10 -> 64 -> 64 -> 1 network (4,929 weights per model) instead of v11
+template <int WARPS, int MINB, bool WIDE = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
@@ -653,23 +683,26 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
-        float const* wsrc = p.weights + size_t(mdl) * NPARAMS;
+        float const* wsrc = p.weights + size_t(mdl) * (WIDE ? NPARAMS_WIDE : NPARAMS);
         if (p.timing && lane == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             p.timing[2 * size_t(sim)] = t;
         }
         FastW fw;
-        load_fast_weights(GlobalW{wsrc}, fw);
-        for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
+        if (!WIDE) {
+            load_fast_weights(GlobalW{wsrc}, fw);
+            for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
+        }
         if (lane == 0) {
+            ws.wglobal = wsrc;
             engine_reset(ws.eng, seed);
             ws.st = Stats{};
         }
         __syncwarp();
         uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move(ws, lut, fw, lane, evals, &p.scratch[1]);
+            Move const mv = search_move<WIDE>(ws, lut, fw, lane, evals, &p.scratch[1]);
             if (mv.none) break;
             if (lane == 0) {
                 if (p.trace) {
@@ -747,6 +780,11 @@ Variant const kVariants[] = {
     {eval_kernel<2, 10>, 2, 10}, {eval_kernel<2, 12>, 2, 12},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
+// the widened network: ~10,000 FP32 operations per candidate, more registers per lane
+Variant const kWideVariants[] = {
+    {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
+};
+constexpr int kDefaultWideVariant = 0;
 constexpr int kDefaultVariant = 1;   // 4 warps, 4 blocks/SM: fastest on the full generation in every autotune run
 
 } // namespace
@@ -780,6 +818,8 @@ struct ta3b_ctx {
     uint32_t* d_scratch = nullptr;
     uint64_t* d_timing = nullptr;
     size_t cap_timing = 0;
+    int wide_variant = -1;            // widened-network kernel, set up on first use
+    uint32_t wide_warps = 0, wide_grid = 0;
     std::string err;
 };
 
@@ -817,19 +857,41 @@ int grow(ta3b_ctx* ctx, T*& ptr, size_t& cap, size_t need, char const* what) {
 int check_sizes(ta3b_ctx* ctx, uint32_t num_islands, uint32_t models_per_island, uint32_t num_params,
                 uint32_t num_games) {
     if (!ctx) return fail(ctx, TA3B_ERR_ARG, "null context");
-    if (num_params != NPARAMS)
-        return fail(ctx, TA3B_ERR_ARG, "num_params must be " + std::to_string(NPARAMS) + " (v11 value model)");
+    if (num_params != NPARAMS && num_params != NPARAMS_WIDE)
+        return fail(ctx, TA3B_ERR_ARG, "num_params must be " + std::to_string(NPARAMS) + " (v11) or " +
+                                           std::to_string(NPARAMS_WIDE) + " (10 -> 64 -> 64 -> 1)");
     uint64_t const sims = uint64_t(num_islands) * models_per_island * num_games;
     if (sims > 0xFFFFFFF0ull) return fail(ctx, TA3B_ERR_ARG, "too many sims in one batch");
     return TA3B_OK;
 }
 
-int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st) {
+int setup_wide(ta3b_ctx* ctx) {
+    if (ctx->wide_variant >= 0) return TA3B_OK;
+    Variant const& v = kWideVariants[kDefaultWideVariant];
+    size_t const dyn = v.warps * sizeof(WarpShared);
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared), "smem carveout");
+    int per_sm = 0;
+    TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
+    if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "widened kernel does not fit on an SM");
+    ctx->wide_variant = kDefaultWideVariant;
+    ctx->wide_warps = v.warps;
+    ctx->wide_grid = ctx->sms * uint32_t(per_sm);
+    return TA3B_OK;
+}
+
+int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, bool wide = false) {
     if (prm.total_sims == 0) return TA3B_OK;
+    if (wide)
+        if (int rc = setup_wide(ctx)) return rc;
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, 2 * sizeof(uint32_t), st), "reset work queue");
-    uint32_t const need_blocks = (prm.total_sims + ctx->warps_per_block - 1) / ctx->warps_per_block;
-    uint32_t const grid = need_blocks < ctx->grid ? need_blocks : ctx->grid;
-    kVariants[ctx->variant].fn<<<grid, ctx->warps_per_block * 32, ctx->warps_per_block * sizeof(WarpShared), st>>>(prm);
+    uint32_t const warps = wide ? ctx->wide_warps : ctx->warps_per_block;
+    uint32_t const max_grid = wide ? ctx->wide_grid : ctx->grid;
+    uint32_t const need_blocks = (prm.total_sims + warps - 1) / warps;
+    uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
+    KernelFn const fn = wide ? kWideVariants[ctx->wide_variant].fn : kVariants[ctx->variant].fn;
+    fn<<<grid, warps * 32, warps * sizeof(WarpShared), st>>>(prm);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     return TA3B_OK;
 }
@@ -853,7 +915,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     if (sims == 0) return TA3B_OK;
     if (!weights || !seeds || !score_out) return fail(ctx, TA3B_ERR_ARG, "null weights / seeds / score_out");
     TA3B_CUDA(ctx, cudaSetDevice(ctx->device), "set device");
-    if (int rc = grow(ctx, ctx->d_w, ctx->cap_w, models * NPARAMS, "alloc weights")) return rc;
+    if (int rc = grow(ctx, ctx->d_w, ctx->cap_w, models * num_params, "alloc weights")) return rc;
     if (int rc = grow(ctx, ctx->d_seeds, ctx->cap_seeds, uint64_t(num_islands) * num_games, "alloc seeds")) return rc;
     if (ctx->cap_sims < sims) {
         size_t c = ctx->cap_sims;
@@ -879,7 +941,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
             ctx->cap_tb = sims;
         }
     }
-    TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * NPARAMS * sizeof(float), cudaMemcpyHostToDevice,
+    TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float), cudaMemcpyHostToDevice,
                                    ctx->stream), "copy weights");
     TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_seeds, seeds, uint64_t(num_islands) * num_games * sizeof(uint64_t),
                                    cudaMemcpyHostToDevice, ctx->stream), "copy seeds");
@@ -899,7 +961,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     prm.models_per_island = mpi;
     prm.max_moves = max_moves;
     prm.total_sims = uint32_t(sims);
-    if (int rc = launch(ctx, prm, ctx->stream)) return rc;
+    if (int rc = launch(ctx, prm, ctx->stream, num_params == NPARAMS_WIDE)) return rc;
     TA3B_CUDA(ctx, cudaMemcpyAsync(score_out, ctx->d_score, sims * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
               "copy score");
     if (pieces_out)
@@ -1064,7 +1126,7 @@ int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands
     prm.models_per_island = models_per_island;
     prm.max_moves = max_moves;
     prm.total_sims = uint32_t(sims);
-    return launch(ctx, prm, stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
+    return launch(ctx, prm, stream ? static_cast<cudaStream_t>(stream) : ctx->stream, num_params == NPARAMS_WIDE);
 }
 
 int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out) {

@@ -15,7 +15,15 @@ import os
 
 import numpy as np
 
-from .workload import NUM_PARAMS
+from .workload import NUM_PARAMS, NUM_PARAMS_WIDE
+
+MODEL_SIZES = (NUM_PARAMS, NUM_PARAMS_WIDE)   # v11 (10 -> 8 -> 1), widened (10 -> 64 -> 64 -> 1)
+
+
+def _rows(weights) -> np.ndarray:
+    """Weights as (models, params): a 2-D array keeps its shape, anything else is v11 rows."""
+    w = np.ascontiguousarray(weights, dtype=np.float32)
+    return w if w.ndim == 2 and w.shape[1] in MODEL_SIZES else w.reshape(-1, NUM_PARAMS)
 
 _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "libta3b.so")
 # TA3B_LIBRARY may name another build of the same C ABI (e.g. an experimental one)
@@ -112,8 +120,8 @@ class ModelEvaluator:
     def _prep(weights, num_models, seeds):
         w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
         s = np.ascontiguousarray(seeds, dtype=np.uint64).reshape(-1)
-        if w.size != num_models * NUM_PARAMS:
-            raise EvaluatorError("weights.size() must equal num_models * NUM_PARAMS")
+        if num_models == 0 or w.size % num_models or w.size // num_models not in MODEL_SIZES:
+            raise EvaluatorError("weights.size() must equal num_models * NUM_PARAMS (97 or 4929)")
         return w, s
 
     def eval(self, weights, num_models: int, seeds, max_moves: int) -> np.ndarray:
@@ -125,21 +133,21 @@ class ModelEvaluator:
         w, s = self._prep(weights, num_models, seeds)
         n = num_models * s.size
         sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
-        self._check(self._lib.ta3b_eval(self._ctx, _p(w), num_models, NUM_PARAMS, _p(s), s.size, max_moves, _p(sc),
-                                        _p(pc), _p(lc)))
+        self._check(self._lib.ta3b_eval(self._ctx, _p(w), num_models, w.size // num_models, _p(s), s.size, max_moves,
+                                        _p(sc), _p(pc), _p(lc)))
         return sc, pc, lc
 
     def eval_islands(self, weights, seeds_per_island, max_moves: int):
         """weights (islands * models_per_island, 97); seeds_per_island (islands, games)."""
         s = np.ascontiguousarray(seeds_per_island, dtype=np.uint64)
         islands, games = s.shape
-        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1, NUM_PARAMS)
+        w = _rows(weights)
         if w.shape[0] % islands:
             raise EvaluatorError("model count must be a multiple of the island count")
         mpi = w.shape[0] // islands
         n = w.shape[0] * games
         sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
-        self._check(self._lib.ta3b_eval_islands(self._ctx, _p(w), islands, mpi, NUM_PARAMS, _p(s), games, max_moves,
+        self._check(self._lib.ta3b_eval_islands(self._ctx, _p(w), islands, mpi, w.shape[1], _p(s), games, max_moves,
                                                 _p(sc), _p(pc), _p(lc)))
         return sc, pc, lc
 
@@ -147,11 +155,11 @@ class ModelEvaluator:
         """Island batch plus per-sim scheduling data: (score, pieces, evals, timing[n, 2] ns)."""
         s = np.ascontiguousarray(seeds_per_island, dtype=np.uint64)
         islands, games = s.shape
-        w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1, NUM_PARAMS)
+        w = _rows(weights)
         n = w.shape[0] * games
         sc, pc, ec = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
         tm = np.zeros((n, 2), np.uint64)
-        self._check(self._lib.ta3b_eval_timed(self._ctx, _p(w), islands, w.shape[0] // islands, NUM_PARAMS, _p(s),
+        self._check(self._lib.ta3b_eval_timed(self._ctx, _p(w), islands, w.shape[0] // islands, w.shape[1], _p(s),
                                               games, max_moves, _p(sc), _p(pc), _p(ec), _p(tm)))
         return sc, pc, ec, tm
 
@@ -162,7 +170,8 @@ class ModelEvaluator:
         out = {"score": np.zeros(n, np.float32), "pieces": np.zeros(n, np.uint32), "lines": np.zeros(n, np.uint32),
                "evals": np.zeros(n, np.uint32), "trace": np.zeros((n, max(max_moves, 1) * 3), np.uint8),
                "moves": np.zeros(n, np.uint32), "board": np.zeros((n, 10), np.uint32)}
-        self._check(self._lib.ta3b_eval_trace(self._ctx, _p(w), num_models, NUM_PARAMS, _p(s), s.size, max_moves,
+        self._check(self._lib.ta3b_eval_trace(self._ctx, _p(w), num_models, w.size // num_models, _p(s), s.size,
+                                              max_moves,
                                               _p(out["score"]), _p(out["pieces"]), _p(out["lines"]),
                                               _p(out["evals"]), _p(out["trace"]), _p(out["moves"]),
                                               _p(out["board"])))
@@ -171,13 +180,14 @@ class ModelEvaluator:
     def eval_device(self, weights, seeds, max_moves: int, score, pieces=None, lines=None, evals=None,
                     num_islands: int = 1, stream=None):
         """Device-resident batch (torch CUDA tensors); enqueued, not synchronised.
-        weights (islands * mpi, 97) float32, seeds (islands, games) uint64 viewed as int64."""
+        weights (islands * mpi, 97 or 4929) float32, seeds (islands, games) uint64 viewed as int64."""
         islands = num_islands
         games = seeds.numel() // islands
-        models = weights.numel() // NUM_PARAMS
+        nparams = weights.shape[-1] if weights.dim() == 2 and weights.shape[-1] in MODEL_SIZES else NUM_PARAMS
+        models = weights.numel() // nparams
         ptr = lambda t: None if t is None else C.c_void_p(t.data_ptr())
         st = C.c_void_p(stream.cuda_stream) if stream is not None else None
-        self._check(self._lib.ta3b_eval_device(self._ctx, ptr(weights), islands, models // islands, NUM_PARAMS,
+        self._check(self._lib.ta3b_eval_device(self._ctx, ptr(weights), islands, models // islands, nparams,
                                                ptr(seeds), games, max_moves, ptr(score), ptr(pieces), ptr(lines),
                                                ptr(evals), st))
 

@@ -22,6 +22,10 @@ import os
 import numpy as np
 
 NUM_PARAMS = 97          # ta3_ai/incl/ta3/ai/models/models/model_v11.hpp:44
+# the reference's dense layers widened to 10 -> 64 -> 64 -> 1 (utility.hpp:29-46 layout per layer:
+# [out][in] weights then [out] biases)
+WIDE_LAYERS = ((10, 64), (64, 64), (64, 1))
+NUM_PARAMS_WIDE = sum(i * o + o for i, o in WIDE_LAYERS)   # 4929
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 _M64 = (1 << 64) - 1
 
@@ -148,3 +152,25 @@ def uneven_batch(models: int = 200, games: int = 100, max_moves: int = 10000, se
     order = np.argsort(splitmix_u64(seed + 7, models), kind="stable")
     seeds = xoshiro_seeds(seed, games)[None, :]
     return Batch(f"{models} models x {games} games (10% champion), cap {max_moves}", w[order], seeds, max_moves)
+
+
+def wide_scale() -> np.ndarray:
+    """Per-parameter standard deviation of the widened network's initialisation:
+    1 / sqrt(fan_in) for weights, 0 for biases."""
+    parts = []
+    for fan_in, fan_out in WIDE_LAYERS:
+        parts.append(np.full(fan_in * fan_out, 1.0 / np.sqrt(fan_in)))
+        parts.append(np.zeros(fan_out))
+    return np.concatenate(parts)
+
+
+def wide_batch(islands: int = 8, pop: int = 100, games: int = 100, max_moves: int = 2000, seed: int = 3) -> Batch:
+    """The widened evaluator's generation: islands x pop models of the 10 -> 64 ->
+    64 -> 1 network, each an independent N(0, 1/fan_in) initialisation drawn from
+    ``seed``; island i plays the ``games`` seeds simulate() derives from seed*1000+i."""
+    z = normal(seed, islands * pop * NUM_PARAMS_WIDE).reshape(islands * pop, NUM_PARAMS_WIDE)
+    sc = wide_scale()
+    w = np.where(sc[None, :] > 0, z * sc[None, :], 0.0).astype(np.float32)   # biases exactly +0
+    seeds = np.stack([xoshiro_seeds(seed * 1000 + i, games) for i in range(islands)])
+    return Batch(f"widened 10-64-64-1: {islands} islands x {pop} x {games} games = {islands * pop * games} sims, "
+                 f"cap {max_moves}", w, seeds, max_moves)
