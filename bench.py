@@ -136,28 +136,31 @@ def _ref_lib(wide: bool = False):
 
 
 def cpu_rate(batch: workload.Batch, budget_s: float, threads: int):
-    """Placements/s of the CPU path over a bounded sample of the batch: whole
-    models of island 0 (each with its island's games), in workload order,
-    `threads` host threads over the (model, game) pairs, until budget_s."""
+    """Placements/s of the CPU path over a bounded sample of the batch: island 0's
+    (model, game) pairs in workload order, `threads` games of one model per call
+    (one host thread each), until budget_s of work."""
     f, kind = _ref_lib(batch.weights.shape[1] == workload.NUM_PARAMS_WIDE)
     p = lambda a: a.ctypes.data_as(C.c_void_p)
     games = batch.games
     mpi = batch.models // batch.islands
-    per_chunk = max(1, threads // games)
-    total_ev, models, t_used = 0, 0, 0.0
-    while t_used < budget_s and models < mpi:
-        c = min(per_chunk, mpi - models)
-        w = np.ascontiguousarray(batch.weights[models:models + c], np.float32)
-        seeds = np.ascontiguousarray(batch.seeds[0], np.uint64)
-        sc = np.zeros(c * games, np.float32)
+    total_ev, sims, t_used = 0, 0, 0.0
+    m, g0 = 0, 0
+    while t_used < budget_s and m < mpi:
+        c = min(threads, games - g0)
+        w = np.ascontiguousarray(batch.weights[m:m + 1], np.float32)
+        seeds = np.ascontiguousarray(batch.seeds[0][g0:g0 + c], np.uint64)
+        sc = np.zeros(c, np.float32)
         evs = C.c_uint64()
         t0 = time.perf_counter()
-        f(p(w), C.c_uint32(c), p(seeds), C.c_uint32(games), C.c_uint32(batch.max_moves), C.c_uint32(threads), p(sc),
+        f(p(w), C.c_uint32(1), p(seeds), C.c_uint32(c), C.c_uint32(batch.max_moves), C.c_uint32(c), p(sc),
           None, None, C.byref(evs))
         t_used += time.perf_counter() - t0
         total_ev += evs.value
-        models += c
-    return total_ev / t_used, kind, models * games, t_used
+        sims += c
+        g0 += c
+        if g0 >= games:
+            m, g0 = m + 1, 0
+    return total_ev / t_used, kind, sims, t_used
 
 
 def host_threads() -> int:

@@ -16,8 +16,9 @@
  * candidates, the surrogate ranks them, and only the best-predicted
  * `surrogate_top` plus `surrogate_random` random others are fully evaluated
  * and told to the optimiser. The surrogate is retrained every
- * `surrogate_retrain` generations on all fully evaluated (parameters -> mean
- * score) pairs except the latest generation, which is held out; while its
+ * `surrogate_retrain` generations on the fully evaluated (parameters -> mean
+ * score) pairs of the last `surrogate_window` generations (all when 0) except
+ * the latest generation, which is held out; while its
  * Spearman rho on that held-out slice is below `surrogate_min_rho` the
  * generation runs without pre-screening. Every fitness the trainer reports
  * comes from full evaluation. */
@@ -70,6 +71,7 @@ typedef struct {
     uint32_t surrogate_epochs;      /* built-in GPU surrogate: epochs per retrain */
     uint32_t surrogate_batch;       /* built-in GPU surrogate: minibatch rows */
     double surrogate_lr;            /* built-in GPU surrogate: Adam learning rate */
+    uint32_t surrogate_window;      /* train on the last N generations before the held-out one (0 = all) */
 } ta3t_config;
 
 typedef struct {

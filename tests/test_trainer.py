@@ -185,3 +185,21 @@ def test_errors_are_reported(host):
         host.Trainer(small(host, population=3), score=quadratic)
     with pytest.raises(RuntimeError):
         host.Trainer(small(host, surrogate_start_gen=2), score=quadratic)     # no surrogate given
+
+
+def test_surrogate_window_limits_the_training_set(host):
+    seen = []
+
+    class Window(Exact):
+        def train(self, x, y):
+            seen.append(len(y))
+
+    c = small(host, surrogate_start_gen=6, surrogate_sample=20, surrogate_top=6, surrogate_random=2,
+               surrogate_retrain=2, surrogate_window=2)
+    t = host.Trainer(c, score=quadratic, surrogate=Window())
+    for _ in range(8):
+        t.run_generation()
+    per_gen = c.islands * c.population
+    # retrains at generations 6 and 8: the two generations before the held-out one
+    assert seen[0] == 2 * per_gen
+    assert seen[1] == per_gen + c.islands * (6 + 2)

@@ -314,7 +314,10 @@ struct ta3t_trainer {
         size_t const P = cfg.num_params;
         std::vector<float> tx, ty, hx;
         std::vector<double> hy;
+        uint64_t const first = cfg.surrogate_window && gen > uint64_t(cfg.surrogate_window) + 1
+                                   ? gen - 1 - cfg.surrogate_window : 0;
         for (size_t i = 0; i < arch_y.size(); ++i) {
+            if (arch_gen[i] < first) continue;
             bool const held = arch_gen[i] + 1 == gen;
             float const* xi = &arch_x[i * P];
             if (held) {
@@ -499,6 +502,7 @@ void ta3t_default_config(ta3t_config* c) {
     c->surrogate_epochs = 40;
     c->surrogate_batch = 256;
     c->surrogate_lr = 1e-3;
+    c->surrogate_window = 0;
 }
 
 static ta3t_trainer* create(const ta3t_config* cfg, std::string const* state, ta3t_score_fn fn, void* user,

@@ -36,7 +36,8 @@ class TrainerConfig(C.Structure):
                 ("surrogate_start_gen", C.c_uint32), ("surrogate_sample", C.c_uint32),
                 ("surrogate_top", C.c_uint32), ("surrogate_random", C.c_uint32),
                 ("surrogate_retrain", C.c_uint32), ("surrogate_min_rho", C.c_double),
-                ("surrogate_epochs", C.c_uint32), ("surrogate_batch", C.c_uint32), ("surrogate_lr", C.c_double)]
+                ("surrogate_epochs", C.c_uint32), ("surrogate_batch", C.c_uint32), ("surrogate_lr", C.c_double),
+                ("surrogate_window", C.c_uint32)]
 
 
 class TrainerStats(C.Structure):
