@@ -120,9 +120,16 @@ class ModelEvaluator:
     def _prep(weights, num_models, seeds):
         w = np.ascontiguousarray(weights, dtype=np.float32).reshape(-1)
         s = np.ascontiguousarray(seeds, dtype=np.uint64).reshape(-1)
-        if num_models == 0 or w.size % num_models or w.size // num_models not in MODEL_SIZES:
+        if num_models == 0:
+            if w.size:
+                raise EvaluatorError("weights given for zero models")
+        elif w.size % num_models or w.size // num_models not in MODEL_SIZES:
             raise EvaluatorError("weights.size() must equal num_models * NUM_PARAMS (97 or 4929)")
         return w, s
+
+    @staticmethod
+    def _nparams(w, num_models) -> int:
+        return w.size // num_models if num_models else NUM_PARAMS
 
     def eval(self, weights, num_models: int, seeds, max_moves: int) -> np.ndarray:
         """Per-(model, game) fitness, model-major (index m * len(seeds) + g)."""
@@ -133,8 +140,8 @@ class ModelEvaluator:
         w, s = self._prep(weights, num_models, seeds)
         n = num_models * s.size
         sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
-        self._check(self._lib.ta3b_eval(self._ctx, _p(w), num_models, w.size // num_models, _p(s), s.size, max_moves,
-                                        _p(sc), _p(pc), _p(lc)))
+        self._check(self._lib.ta3b_eval(self._ctx, _p(w), num_models, self._nparams(w, num_models), _p(s), s.size,
+                                        max_moves, _p(sc), _p(pc), _p(lc)))
         return sc, pc, lc
 
     def eval_islands(self, weights, seeds_per_island, max_moves: int):
@@ -170,7 +177,7 @@ class ModelEvaluator:
         out = {"score": np.zeros(n, np.float32), "pieces": np.zeros(n, np.uint32), "lines": np.zeros(n, np.uint32),
                "evals": np.zeros(n, np.uint32), "trace": np.zeros((n, max(max_moves, 1) * 3), np.uint8),
                "moves": np.zeros(n, np.uint32), "board": np.zeros((n, 10), np.uint32)}
-        self._check(self._lib.ta3b_eval_trace(self._ctx, _p(w), num_models, w.size // num_models, _p(s), s.size,
+        self._check(self._lib.ta3b_eval_trace(self._ctx, _p(w), num_models, self._nparams(w, num_models), _p(s), s.size,
                                               max_moves,
                                               _p(out["score"]), _p(out["pieces"]), _p(out["lines"]),
                                               _p(out["evals"]), _p(out["trace"]), _p(out["moves"]),
