@@ -52,10 +52,9 @@ METRIC_WIDE = ("beam placements/s on 1 B200 (widened 10-64-64-1 evaluator: 8 isl
                "= 80k sims, cap 2000)")
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
 # on the small-case capture) and its DRAM bytes per full-generation launch
-# (ncu dram__bytes_read.sum + dram__bytes_write.sum, captured at 200 and 800 sims:
-# 204,800 and 722,944 bytes read, 0 written -> 864 B per sim + 32 KB, scaled to 10,000 sims).
+# (ncu dram__bytes_read.sum + dram__bytes_write.sum, 1-pass capture of the full launch).
 LANE_INSTR_PER_PLACEMENT = 564
-DRAM_BYTES_PER_LAUNCH = 8_670_000
+DRAM_BYTES_PER_LAUNCH = 888_576
 
 
 from tetris_ai3_b200.dist import rank_env as _dist_env, rank_seed, reduce_timing  # noqa: E402

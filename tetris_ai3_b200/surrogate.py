@@ -103,3 +103,34 @@ class Surrogate:
         lv = np.empty(n, np.float32) if with_logvar else None
         self._ok(self.lib.ta3s_predict(self.h, _p(x), n, _p(mean), _p(lv)))
         return (mean, lv) if with_logvar else mean
+
+
+def main(argv=None):
+    """Time the GPU surrogate on a seeded synthetic (parameters -> score) set:
+    python -m tetris_ai3_b200.surrogate [--rows 8000] [--epochs 40] [--batch 256]"""
+    import argparse
+    import json
+    import time
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rows", type=int, default=8000)
+    ap.add_argument("--epochs", type=int, default=40)
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--predict", type=int, default=800)
+    args = ap.parse_args(argv)
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=(8, 97)) / np.sqrt(97)
+    x = rng.normal(size=(args.rows, 97)).astype(np.float32)
+    y = (-((x @ a.T) ** 2).sum(1)).astype(np.float32)
+    s = Surrogate(batch=args.batch, epochs=args.epochs)
+    t0 = time.perf_counter()
+    loss = s.train(x, y)
+    t1 = time.perf_counter()
+    s.predict(x[:args.predict])
+    t2 = time.perf_counter()
+    steps = args.epochs * ((args.rows + args.batch - 1) // args.batch)
+    print(json.dumps({"rows": args.rows, "epochs": args.epochs, "batch": args.batch, "train_s": t1 - t0,
+                      "ms_per_step": 1e3 * (t1 - t0) / steps, "predict_ms": 1e3 * (t2 - t1), "final_loss": loss}))
+
+
+if __name__ == "__main__":
+    main()
