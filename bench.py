@@ -48,6 +48,8 @@ REF_OPS_PER_PLACEMENT = 1010
 # The widened 10 -> 64 -> 64 -> 1 network replaces the MLP's 192 by
 # 64 x (10 mul + 10 add + relu) + 64 x (64 mul + 64 add + relu) + 64 mul + 64 add = 9,728.
 REF_OPS_PER_PLACEMENT_WIDE = 1010 - 192 + 9728
+METRIC_STRESS = ("beam placements/s on 1 B200 (uneven-length stress: 200 models x 100 games = 20k sims, "
+                 "10% v11 champion, cap 10000)")
 METRIC_WIDE = ("beam placements/s on 1 B200 (widened 10-64-64-1 evaluator: 8 islands x 100 models x 100 games "
                "= 80k sims, cap 2000)")
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
@@ -171,6 +173,9 @@ def host_threads() -> int:
 
 def _batch(args, rank: int = 0) -> workload.Batch:
     """The workload of one rank (weak scaling: rank r scores generation seed base+r)."""
+    if args.model == "stress":
+        return workload.uneven_batch(models=args.pop or 200, games=args.games or 100, max_moves=args.cap or 10000,
+                                     seed=rank_seed(2, rank))
     if args.model == "wide":
         return workload.wide_batch(islands=args.islands or 8, pop=args.pop or 100, games=args.games or 100,
                                    max_moves=args.cap or 2000, seed=rank_seed(3, rank))
@@ -183,7 +188,7 @@ def run_reference(args):
     if rank != 0:
         return
     batch = _batch(args)
-    metric = METRIC_WIDE if args.model == "wide" else METRIC
+    metric = {"wide": METRIC_WIDE, "stress": METRIC_STRESS}.get(args.model, METRIC)
     threads = host_threads()
     rates = []
     kind = "reference"
@@ -229,7 +234,7 @@ def run_ours(args):
     # weak scaling: each rank scores its own generation (islands seeded per rank)
     batch = _batch(args, rank)
     wide = args.model == "wide"
-    metric = METRIC_WIDE if wide else METRIC
+    metric = {"wide": METRIC_WIDE, "stress": METRIC_STRESS}.get(args.model, METRIC)
     ops_per_placement = REF_OPS_PER_PLACEMENT_WIDE if wide else REF_OPS_PER_PLACEMENT
     ev = ModelEvaluator(device=local)
     stream = torch.cuda.Stream(device=dev)
@@ -358,8 +363,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="fixed kernel variant (default: autotune)")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--model", choices=["v11", "wide"], default="v11",
-                    help="v11 (headline) or the widened 10-64-64-1 evaluator's 80k-sim generation")
+    ap.add_argument("--model", choices=["v11", "wide", "stress"], default="v11",
+                    help="v11 (headline), the widened 10-64-64-1 evaluator's 80k-sim generation, or the "
+                         "uneven-length stress batch (20k sims, 10%% champion, cap 10000)")
     # reduced shapes for profiling captures only (the headline is the default full generation)
     ap.add_argument("--islands", type=int, default=0)
     ap.add_argument("--pop", type=int, default=0)

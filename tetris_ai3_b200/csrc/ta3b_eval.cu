@@ -778,6 +778,8 @@ struct Variant {
 Variant const kVariants[] = {
     {eval_kernel<4, 3>, 4, 3}, {eval_kernel<4, 4>, 4, 4}, {eval_kernel<4, 5>, 4, 5}, {eval_kernel<4, 6>, 4, 6},
     {eval_kernel<2, 10>, 2, 10}, {eval_kernel<2, 12>, 2, 12},
+    // larger blocks (8 and 16 games per block, 256 / 512 threads), same 128-register cap
+    {eval_kernel<8, 2>, 8, 2}, {eval_kernel<16, 1>, 16, 1},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // the widened network: ~10,000 FP32 operations per candidate, more registers per lane
