@@ -230,6 +230,10 @@ constexpr int WH = 64;
 constexpr int WIDE_B1 = NIN * WH, WIDE_W2 = WIDE_B1 + WH, WIDE_B2 = WIDE_W2 + WH * WH, WIDE_W3 = WIDE_B2 + WH,
               WIDE_B3 = WIDE_W3 + WH, NPARAMS_WIDE = WIDE_B3 + 1;
 static_assert(NPARAMS_WIDE == 4929, "10 -> 64 -> 64 -> 1");
+// device copies of widened models are padded to a 16-byte multiple, so layer 2's rows
+// (which start at WIDE_W2 = 768 floats) can be read with 16-byte loads
+constexpr int WIDE_STRIDE = 4932;
+static_assert(WIDE_STRIDE % 4 == 0 && WIDE_STRIDE >= NPARAMS_WIDE && WIDE_W2 % 4 == 0 && WH % 4 == 0, "alignment");
 
 TA3B_HD float relu(float v) { return v > 0.0f ? v : 0.0f; }    // std::max<float>(0, v)
 
@@ -251,12 +255,37 @@ TA3B_HD float wide_forward(float const (&in)[NIN], WF const& w) {
     for (int o = 0; o < WH; o += 4) {
         float a = w(WIDE_B2 + o), b = w(WIDE_B2 + o + 1), c = w(WIDE_B2 + o + 2), d = w(WIDE_B2 + o + 3);
         int const r = WIDE_W2 + o * WH;
+        if (WF::VEC4) {
+            // 16-byte loads of four consecutive weights of each row; the sums keep the reference order
 #pragma unroll
-        for (int i = 0; i < WH; ++i) {
-            a = f_add(a, f_mul(h1[i], w(r + i)));
-            b = f_add(b, f_mul(h1[i], w(r + WH + i)));
-            c = f_add(c, f_mul(h1[i], w(r + 2 * WH + i)));
-            d = f_add(d, f_mul(h1[i], w(r + 3 * WH + i)));
+            for (int i = 0; i < WH; i += 4) {
+                auto const qa = w.v4(r + i), qb = w.v4(r + WH + i), qc = w.v4(r + 2 * WH + i),
+                           qd = w.v4(r + 3 * WH + i);
+                a = f_add(a, f_mul(h1[i], qa.x));
+                b = f_add(b, f_mul(h1[i], qb.x));
+                c = f_add(c, f_mul(h1[i], qc.x));
+                d = f_add(d, f_mul(h1[i], qd.x));
+                a = f_add(a, f_mul(h1[i + 1], qa.y));
+                b = f_add(b, f_mul(h1[i + 1], qb.y));
+                c = f_add(c, f_mul(h1[i + 1], qc.y));
+                d = f_add(d, f_mul(h1[i + 1], qd.y));
+                a = f_add(a, f_mul(h1[i + 2], qa.z));
+                b = f_add(b, f_mul(h1[i + 2], qb.z));
+                c = f_add(c, f_mul(h1[i + 2], qc.z));
+                d = f_add(d, f_mul(h1[i + 2], qd.z));
+                a = f_add(a, f_mul(h1[i + 3], qa.w));
+                b = f_add(b, f_mul(h1[i + 3], qb.w));
+                c = f_add(c, f_mul(h1[i + 3], qc.w));
+                d = f_add(d, f_mul(h1[i + 3], qd.w));
+            }
+        } else {
+#pragma unroll
+            for (int i = 0; i < WH; ++i) {
+                a = f_add(a, f_mul(h1[i], w(r + i)));
+                b = f_add(b, f_mul(h1[i], w(r + WH + i)));
+                c = f_add(c, f_mul(h1[i], w(r + 2 * WH + i)));
+                d = f_add(d, f_mul(h1[i], w(r + 3 * WH + i)));
+            }
         }
         out = f_add(out, f_mul(relu(a), w(WIDE_W3 + o)));
         out = f_add(out, f_mul(relu(b), w(WIDE_W3 + o + 1)));

@@ -198,12 +198,21 @@ __device__ int engine_place(Engine& e, int o, int x) {                       // 
 
 // ------------------------------------------------------------ candidates ---
 struct SmemW {                       // weights read from shared memory (broadcast loads)
+    static constexpr bool VEC4 = false;
     float const* p;
     __device__ __forceinline__ float operator()(int i) const { return p[i]; }
 };
 struct GlobalW {
+    static constexpr bool VEC4 = false;
     float const* p;
     __device__ __forceinline__ float operator()(int i) const { return __ldg(p + i); }
+};
+// a widened model's padded device copy (16-byte aligned, WIDE_STRIDE floats per model)
+struct WideW {
+    static constexpr bool VEC4 = true;
+    float const* p;
+    __device__ __forceinline__ float operator()(int i) const { return __ldg(p + i); }
+    __device__ __forceinline__ float4 v4(int i) const { return __ldg(reinterpret_cast<float4 const*>(p + i)); }
 };
 
 __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uint32_t (&b)[W]) {
@@ -254,7 +263,7 @@ __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ 
     r.h4 = sp.x;
     r.hm4 = sp.y;
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
-    return fast_eval_wide(r, rec[R_CLEARS], pf, held_i, GlobalW{w}, v);
+    return fast_eval_wide(r, rec[R_CLEARS], pf, held_i, WideW{w}, v);
 }
 
 // stats_v4::advance (tetris_stats.hpp:19-23 with metrics.hpp:196-229)
@@ -388,7 +397,7 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
     int cl = 0;
     if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return 0;
     BoardInts const bi = board_ints(nb);
-    float const v = WIDE ? value_full_wide(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, GlobalW{ws->wglobal})
+    float const v = WIDE ? value_full_wide(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, WideW{ws->wglobal})
                          : value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
     return candidate_key(leaf, v, info, i);
 }
@@ -683,7 +692,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
-        float const* wsrc = p.weights + size_t(mdl) * (WIDE ? NPARAMS_WIDE : NPARAMS);
+        float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WIDE_STRIDE : NPARAMS);
         if (p.timing && lane == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -768,6 +777,14 @@ __global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand,
     full_v[t] = full_legal[t] ? value_full(rec[R_CLEARS] + clear_bump(cl), board_ints(nb), held, GlobalW{w}) : 0.0f;
 }
 
+// widened models -> their padded device layout (WIDE_STRIDE floats per model)
+__global__ void repack_wide_kernel(float const* __restrict__ src, uint32_t models, float* __restrict__ dst) {
+    size_t const i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= size_t(models) * WIDE_STRIDE) return;
+    size_t const m = i / WIDE_STRIDE, j = i % WIDE_STRIDE;
+    dst[i] = j < size_t(NPARAMS_WIDE) ? src[m * NPARAMS_WIDE + j] : 0.0f;
+}
+
 // Launch-shape variants (warps per block, minimum resident blocks per SM =
 // the register cap): the autotuner's search space.
 using KernelFn = void (*)(Params);
@@ -820,6 +837,8 @@ struct ta3b_ctx {
     uint32_t* d_scratch = nullptr;
     uint64_t* d_timing = nullptr;
     size_t cap_timing = 0;
+    float* d_wpad = nullptr;          // widened models in their padded device layout
+    size_t cap_wpad = 0;
     int wide_variant = -1;            // widened-network kernel, set up on first use
     uint32_t wide_warps = 0, wide_grid = 0;
     std::string err;
@@ -917,7 +936,8 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     if (sims == 0) return TA3B_OK;
     if (!weights || !seeds || !score_out) return fail(ctx, TA3B_ERR_ARG, "null weights / seeds / score_out");
     TA3B_CUDA(ctx, cudaSetDevice(ctx->device), "set device");
-    if (int rc = grow(ctx, ctx->d_w, ctx->cap_w, models * num_params, "alloc weights")) return rc;
+    if (num_params == NPARAMS)
+        if (int rc = grow(ctx, ctx->d_w, ctx->cap_w, models * num_params, "alloc weights")) return rc;
     if (int rc = grow(ctx, ctx->d_seeds, ctx->cap_seeds, uint64_t(num_islands) * num_games, "alloc seeds")) return rc;
     if (ctx->cap_sims < sims) {
         size_t c = ctx->cap_sims;
@@ -943,12 +963,20 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
             ctx->cap_tb = sims;
         }
     }
-    TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float), cudaMemcpyHostToDevice,
-                                   ctx->stream), "copy weights");
+    bool const wide = num_params == NPARAMS_WIDE;
+    if (wide) {
+        if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * WIDE_STRIDE, "alloc padded weights")) return rc;
+        TA3B_CUDA(ctx, cudaMemcpy2DAsync(ctx->d_wpad, WIDE_STRIDE * sizeof(float), weights, NPARAMS_WIDE * sizeof(float),
+                                         NPARAMS_WIDE * sizeof(float), models, cudaMemcpyHostToDevice, ctx->stream),
+                  "copy weights");
+    } else {
+        TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float),
+                                       cudaMemcpyHostToDevice, ctx->stream), "copy weights");
+    }
     TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_seeds, seeds, uint64_t(num_islands) * num_games * sizeof(uint64_t),
                                    cudaMemcpyHostToDevice, ctx->stream), "copy seeds");
     Params prm{};
-    prm.weights = ctx->d_w;
+    prm.weights = wide ? ctx->d_wpad : ctx->d_w;
     prm.seeds = ctx->d_seeds;
     prm.score = ctx->d_score;
     prm.pieces = ctx->d_pieces;
@@ -1072,7 +1100,7 @@ void ta3b_destroy(ta3b_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     void* bufs[] = {ctx->d_w, ctx->d_seeds, ctx->d_score, ctx->d_pieces, ctx->d_lines, ctx->d_evals,
-                    ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing};
+                    ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing, ctx->d_wpad};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1116,8 +1144,17 @@ int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands
     uint64_t const sims = uint64_t(num_islands) * models_per_island * num_games;
     if (sims == 0) return TA3B_OK;
     if (!d_weights || !d_seeds || !d_score) return fail(ctx, TA3B_ERR_ARG, "null device pointer");
+    cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+    bool const wide = num_params == NPARAMS_WIDE;
+    if (wide) {   // the padded copy (allocated on the first widened call of this size)
+        uint64_t const models = uint64_t(num_islands) * models_per_island;
+        if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * WIDE_STRIDE, "alloc padded weights")) return rc;
+        uint64_t const n = models * WIDE_STRIDE;
+        repack_wide_kernel<<<uint32_t((n + 255) / 256), 256, 0, st>>>(d_weights, uint32_t(models), ctx->d_wpad);
+        TA3B_CUDA(ctx, cudaGetLastError(), "repack widened weights");
+    }
     Params prm{};
-    prm.weights = d_weights;
+    prm.weights = wide ? ctx->d_wpad : d_weights;
     prm.seeds = d_seeds;
     prm.score = d_score;
     prm.pieces = d_pieces;
@@ -1128,7 +1165,7 @@ int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands
     prm.models_per_island = models_per_island;
     prm.max_moves = max_moves;
     prm.total_sims = uint32_t(sims);
-    return launch(ctx, prm, stream ? static_cast<cudaStream_t>(stream) : ctx->stream, num_params == NPARAMS_WIDE);
+    return launch(ctx, prm, st, wide);
 }
 
 int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out) {
