@@ -804,7 +804,7 @@ Variant const kWideVariants[] = {
     {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
 };
 constexpr int kDefaultWideVariant = 0;
-constexpr int kDefaultVariant = 1;   // 4 warps, 4 blocks/SM: fastest on the full generation in every autotune run
+constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
 } // namespace
 } // namespace ta3b
