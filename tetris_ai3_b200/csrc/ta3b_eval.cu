@@ -804,6 +804,7 @@ Variant const kWideVariants[] = {
     {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
 };
 constexpr int kDefaultWideVariant = 0;
+constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
 } // namespace
@@ -1295,7 +1296,7 @@ extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_isl
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
         return fail_static(TA3B_ERR_CUDA, "cudaGetDevice failed or device ordinal too large");
-    Variant const& var = kVariants[kDefaultVariant];
+    Variant const& var = kVariants[kNoAllocVariant];
     size_t const dyn = var.warps * sizeof(WarpShared);
     {
         // once per device, with that device current: resolve the scratch array's
