@@ -19,6 +19,7 @@
 #include <numeric>
 #include <random>
 #include <string>
+#include <thread>
 #include <vector>
 
 using namespace ta3b::host;
@@ -58,6 +59,21 @@ struct Xoshiro {
         return r;
     }
 };
+
+// fn(i) for i in [0, n) on up to n host threads (the islands' optimisers are
+// independent, so the result does not depend on the interleaving)
+template<class F>
+void for_islands(uint32_t n, F const& fn) {
+    if (n <= 1) {
+        for (uint32_t i = 0; i < n; ++i) fn(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(n - 1);
+    for (uint32_t i = 1; i < n; ++i) th.emplace_back([&fn, i] { fn(i); });
+    fn(0);
+    for (auto& t : th) t.join();
+}
 
 // Spearman rank correlation (average ranks for ties)
 std::vector<double> ranks(std::vector<double> const& v) {
@@ -358,7 +374,7 @@ struct ta3t_trainer {
         uint32_t const n_ask = pre ? cfg.surrogate_sample : N;
 
         std::vector<double> asked(size_t(I) * n_ask * P);
-        for (uint32_t i = 0; i < I; ++i) islands[i].cma->ask(int(n_ask), &asked[size_t(i) * n_ask * P]);
+        for_islands(I, [&](uint32_t i) { islands[i].cma->ask(int(n_ask), &asked[size_t(i) * n_ask * P]); });
 
         // which candidates get full evaluation
         std::vector<std::vector<int>> chosen(I);
@@ -404,16 +420,16 @@ struct ta3t_trainer {
             }
         if (score(total, xs.data(), fit.data(), means.data())) return 1;
 
-        row = 0;
-        for (uint32_t i = 0; i < I; ++i) {
+        std::vector<size_t> first_row(I + 1, 0);
+        for (uint32_t i = 0; i < I; ++i) first_row[i + 1] = first_row[i] + chosen[i].size();
+        for_islands(I, [&](uint32_t i) {
             Island& is = islands[i];
-            size_t const k = chosen[i].size();
+            size_t const k = chosen[i].size(), r0 = first_row[i];
             is.x.assign(k, vec(P));
             is.f.assign(k, 0.0);
-            for (size_t j = 0; j < k; ++j) is.set_xf(j, &xs[(row + j) * P], fit[row + j]);
-            is.cma->tell(int(k), chosen[i].data(), &fit[row]);
-            row += k;
-        }
+            for (size_t j = 0; j < k; ++j) is.set_xf(j, &xs[(r0 + j) * P], fit[r0 + j]);
+            is.cma->tell(int(k), chosen[i].data(), &fit[r0]);
+        });
         if (pre) {
             std::vector<float> xf(total * P);
             for (size_t k = 0; k < xf.size(); ++k) xf[k] = float(xs[k]);
