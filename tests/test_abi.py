@@ -56,8 +56,8 @@ def test_variants_enumerate(lib):
     from tetris_ai3_b200 import ModelEvaluator
     v = ModelEvaluator.variants()
     assert len(v) == lib.ta3b_num_variants() >= 2
-    assert all(x["warps_per_block"] in (2, 4, 8, 16) for x in v)
-    assert {x["warps_per_block"] for x in v} == {2, 4, 8, 16}
+    assert all(x["warps_per_block"] in (2, 4, 8, 10, 16, 20) for x in v)
+    assert {x["warps_per_block"] for x in v} == {2, 4, 8, 10, 16, 20}
 
 
 def _has_gpu():

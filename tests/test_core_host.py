@@ -58,7 +58,7 @@ def test_full_and_fast_paths_match_oracle(core, oracle):
     rng = np.random.default_rng(11)
     from tetris_ai3_b200 import workload
     ws = [(s * workload.normal(500 + k, 97)).astype(np.float32) for k, s in enumerate([0.5, 2.0, 40.0])]
-    rec = np.zeros(84, np.uint32)
+    rec = np.zeros(core.ta3bt_rec_words(), np.uint32)
     out = np.zeros(10, np.uint32)
     feats = np.zeros(10, np.float32)
     n_fast = n_defer = n_legal = 0
@@ -104,7 +104,7 @@ def test_full_and_fast_paths_match_oracle(core, oracle):
 def test_fast_path_does_not_defer_plain_drops(core):
     # empty board, no piece reaches a row, nothing clears: every placement is fast
     w = np.ones(97, np.float32)
-    rec = np.zeros(84, np.uint32)
+    rec = np.zeros(core.ta3bt_rec_words(), np.uint32)
     core.ta3bt_build_record(ptr(np.zeros(10, np.uint32)), C.c_uint32(0), ptr(w), ptr(rec))
     v = C.c_float()
     for p in range(7):

@@ -145,7 +145,8 @@ def test_device_core_matches_host_core(ev):
     rng = np.random.default_rng(3)
     w = (0.5 * workload.normal(77, 97)).astype(np.float32)
     bds = [b for b in boards(rng, 120) if not (int(np.bitwise_and.reduce(b)) & ((1 << 23) - 1))]
-    recs = np.zeros((len(bds), 84), np.uint32)
+    host.ta3bt_rec_words.restype = C.c_uint32
+    recs = np.zeros((len(bds), host.ta3bt_rec_words()), np.uint32)
     for k, b in enumerate(bds):
         clears = int(rng.integers(0, 3)) | (int(rng.integers(0, 2)) << 16)
         host.ta3bt_build_record(ptr(b), C.c_uint32(clears), ptr(w), ptr(recs[k]))

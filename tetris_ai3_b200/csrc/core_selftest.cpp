@@ -15,6 +15,8 @@ struct HostW {
 
 extern "C" {
 
+uint32_t ta3bt_rec_words() { return uint32_t(ta3b::REC_WORDS); }
+
 void ta3bt_build_record(uint32_t const* b10, uint32_t clears, float const* w97, uint32_t* rec) {
     uint32_t b[ta3b::W];
     for (int x = 0; x < ta3b::W; ++x) b[x] = b10[x];
@@ -34,9 +36,7 @@ int ta3bt_fast(uint32_t const* rec, uint32_t piece, uint32_t idx, int held, floa
     r.rc1 = rec[ta3b::R_RC + 1];
     r.rc2 = rec[ta3b::R_RC + 2];
     ta3b::PlaceFast const pf = ta3b::FAST.place[piece][idx];
-    int const c0 = int((pf.m >> 27) & 0xFu);
-    r.h4 = rec[ta3b::R_SPAN + 2 * c0];
-    r.hm4 = rec[ta3b::R_SPAN + 2 * c0 + 1];
+    ta3b::span_of(rec, int((pf.m >> 27) & 0xFu), r.h4, r.hm4);
     r.combo = rec[ta3b::R_COMBO + ((pf.m >> 16) & 63u)];
     return ta3b::fast_eval<ta3b::MLP_SCALAR>(r, pf, held != 0, fw, *value, dbg);
 }
@@ -138,8 +138,7 @@ Cand candidate(uint32_t const* rec, int piece, int i, bool held, bool leaf, uint
     RecView r;
     for (int o = 0; o < NHID; ++o) __builtin_memcpy(&r.P[o], &rec[R_P + o], 4);
     r.tot = rec[R_TOT]; r.hd = rec[R_HD]; r.rc0 = rec[R_RC]; r.rc1 = rec[R_RC + 1]; r.rc2 = rec[R_RC + 2];
-    int const c0 = int((pf.m >> 27) & 0xFu);
-    r.h4 = rec[R_SPAN + 2 * c0]; r.hm4 = rec[R_SPAN + 2 * c0 + 1];
+    span_of(rec, int((pf.m >> 27) & 0xFu), r.h4, r.hm4);
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
     float v;
     bool const fast = fast_eval<MLP_SCALAR>(r, pf, held, fw, v) == FAST_OK;
@@ -221,9 +220,14 @@ void ta3bt_root_record(uint32_t const* b10, float const* w97, uint32_t* rec) {
     for (int lane = 0; lane < 32; ++lane) {
         ColumnData c;
         column_data(b, c);
-        if (lane < W) {
-            rec[R_BOARD + lane] = b[lane];
-            span_words(c, lane, rec[R_SPAN + 2 * lane], rec[R_SPAN + 2 * lane + 1]);
+        if (lane < W) rec[R_BOARD + lane] = b[lane];
+        if (lane == 22) {
+            uint32_t hb[4], hmb[4];
+            span_bytes(c, hb, hmb);
+            for (int q = 0; q < 4; ++q) {
+                rec[R_HB + q] = hb[q];
+                rec[R_HMB + q] = hmb[q];
+            }
         }
         for (int id = lane; id < NCOMBO; id += 32) {
             int c0, wd;

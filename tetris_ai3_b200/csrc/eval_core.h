@@ -387,21 +387,22 @@ TA3B_HD int dot4_s8(uint32_t a, uint32_t b) {                   // sum of 4 sign
 }
 
 // ------------------------------------------------------ parent record ---
-// One kept frontier node (or the committed board), in 84 u32 words (80 used;
-// the padding staggers the records across shared-memory banks):
-constexpr int REC_WORDS = 84;
+// One kept frontier node (or the committed board), in 68 u32 words (a 16-byte
+// multiple; 68 = 4 mod 32 staggers the records across shared-memory banks):
+constexpr int REC_WORDS = 68;
 constexpr int R_P = 0;        // float[8]: hidden partial sums after the 4 clear inputs
 constexpr int R_BOARD = 8;    // 10 bit-columns
 constexpr int R_CLEARS = 18;  // path clear histogram (4 x 8-bit lanes)
 constexpr int R_TOT = 19;     // holes (8) | max height (5) << 8 | wells (4) << 13 | surface sum (13) << 17
 constexpr int R_HD = 20;      // hole depths total
 constexpr int R_RC = 21;      // 3 words: occupied cells per row, 4 bits per row, rows 0..22
-constexpr int R_SPAN = 24;    // 10 x 2 words, for window origin c0: heights of columns c0..c0+3
-                              // (bytes, 0 past the edge), then (holes - height) of the same columns (signed bytes)
-constexpr int R_COMBO = 44;   // 34 words, per (c0, width) combo: the old surface terms of the window's pairs (12)
+constexpr int R_HB = 24;      // 4 words: column heights as bytes (byte x = column x, bytes 10..15 zero)
+constexpr int R_HMB = 28;     // 4 words: (holes - height) per column as signed bytes (bytes 10..15 zero)
+constexpr int R_COMBO = 32;   // 34 words, per (c0, width) combo: the old surface terms of the window's pairs (12)
                               // | old wells of the window's columns (3) << 12 | left-well precondition << 15
                               // | height of column c0-1 (5) << 16 | right-well precondition << 21
                               // | height of column c0+w (5) << 22
+static_assert(R_COMBO + NCOMBO <= REC_WORDS && REC_WORDS % 4 == 0, "record layout");
 constexpr uint32_t WALL = 31; // height outside the board: satisfies every well-edge rule
 
 // Column data a record is derived from: heights with walls (h[x + 2] = column x),
@@ -465,16 +466,30 @@ TA3B_HD uint32_t row_counts(uint32_t const (&b)[W], int q) {
            (spread(s3 >> (8 * q)) << 3);
 }
 
-TA3B_HD void span_words(ColumnData const& c, int c0, uint32_t& h4, uint32_t& hm4) {
-    h4 = hm4 = 0;
+// the byte arrays R_HB / R_HMB of a record
+TA3B_HD void span_bytes(ColumnData const& c, uint32_t (&hb)[4], uint32_t (&hmb)[4]) {
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        int const x = c0 + i;
-        if (x < W) {
-            h4 |= uint32_t(c.h[x + 2]) << (8 * i);
-            hm4 |= (uint32_t(c.ho[x] - c.h[x + 2]) & 0xFFu) << (8 * i);
-        }
+    for (int q = 0; q < 4; ++q) hb[q] = hmb[q] = 0;
+#pragma unroll
+    for (int x = 0; x < W; ++x) {
+        hb[x >> 2] |= uint32_t(c.h[x + 2]) << (8 * (x & 3));
+        hmb[x >> 2] |= (uint32_t(c.ho[x] - c.h[x + 2]) & 0xFFu) << (8 * (x & 3));
     }
+}
+
+TA3B_HD uint32_t fshr32(uint32_t lo, uint32_t hi, uint32_t sh) {     // low word of (hi:lo) >> sh, sh < 32
+#if defined(__CUDA_ARCH__)
+    return __funnelshift_r(lo, hi, sh);
+#else
+    return sh ? (lo >> sh) | (hi << (32u - sh)) : lo;
+#endif
+}
+
+// window words for origin c0: bytes i = column c0+i (0 past the edge) of the two byte arrays
+TA3B_HD void span_of(uint32_t const* rec, int c0, uint32_t& h4, uint32_t& hm4) {
+    uint32_t const wi = uint32_t(c0) >> 2, sh = (uint32_t(c0) & 3u) * 8u;
+    h4 = fshr32(rec[R_HB + wi], rec[R_HB + wi + 1], sh);
+    hm4 = fshr32(rec[R_HMB + wi], rec[R_HMB + wi + 1], sh);
 }
 
 TA3B_HD uint32_t combo_word(ColumnData const& c, int c0, int wd) {
@@ -526,8 +541,13 @@ TA3B_HD void build_record(uint32_t const (&b)[W], uint32_t clear_bits, WF const&
 #pragma unroll
     for (int q = 0; q < 3; ++q) rec[R_RC + q] = row_counts(b, q);
     // fully unrolled: every column index is a constant, so the column data stays in registers
+    uint32_t hb[4], hmb[4];
+    span_bytes(c, hb, hmb);
 #pragma unroll
-    for (int c0 = 0; c0 < W; ++c0) span_words(c, c0, rec[R_SPAN + 2 * c0], rec[R_SPAN + 2 * c0 + 1]);
+    for (int q = 0; q < 4; ++q) {
+        rec[R_HB + q] = hb[q];
+        rec[R_HMB + q] = hmb[q];
+    }
 #pragma unroll
     for (int id = 0; id < NCOMBO; ++id) {
         int c0, wd;

@@ -243,10 +243,7 @@ __device__ __forceinline__ int fast_candidate(uint32_t const* __restrict__ rec, 
     uint4 const q = *reinterpret_cast<uint4 const*>(rec + R_HD);       // hd, rc0, rc1, rc2
     r.hd = q.x; r.rc0 = q.y; r.rc1 = q.z; r.rc2 = q.w;
     r.tot = rec[R_TOT];
-    uint32_t const c0 = (pf.m >> 27) & 0xFu;
-    uint2 const sp = *reinterpret_cast<uint2 const*>(rec + R_SPAN + 2 * c0);
-    r.h4 = sp.x;
-    r.hm4 = sp.y;
+    span_of(rec, int((pf.m >> 27) & 0xFu), r.h4, r.hm4);
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
     return fast_eval<MLP>(r, pf, held_i, fw, v, dbg);
 }
@@ -258,10 +255,7 @@ __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ 
     uint4 const q = *reinterpret_cast<uint4 const*>(rec + R_HD);
     r.hd = q.x; r.rc0 = q.y; r.rc1 = q.z; r.rc2 = q.w;
     r.tot = rec[R_TOT];
-    uint32_t const c0 = (pf.m >> 27) & 0xFu;
-    uint2 const sp = *reinterpret_cast<uint2 const*>(rec + R_SPAN + 2 * c0);
-    r.h4 = sp.x;
-    r.hm4 = sp.y;
+    span_of(rec, int((pf.m >> 27) & 0xFu), r.h4, r.hm4);
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
     return fast_eval_wide(r, rec[R_CLEARS], pf, held_i, WideW{w}, v);
 }
@@ -797,6 +791,8 @@ Variant const kVariants[] = {
     {eval_kernel<2, 10>, 2, 10}, {eval_kernel<2, 12>, 2, 12},
     // larger blocks (8 and 16 games per block, 256 / 512 threads), same 128-register cap
     {eval_kernel<8, 2>, 8, 2}, {eval_kernel<16, 1>, 16, 1},
+    // 20 warps per SM (the 68-word records leave room for them) at a ~100-register cap
+    {eval_kernel<10, 2>, 10, 2}, {eval_kernel<20, 1>, 20, 1},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // the widened network: ~10,000 FP32 operations per candidate, more registers per lane
