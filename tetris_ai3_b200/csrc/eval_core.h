@@ -238,8 +238,13 @@ static_assert(WIDE_STRIDE % 4 == 0 && WIDE_STRIDE >= NPARAMS_WIDE && WIDE_W2 % 4
 TA3B_HD float relu(float v) { return v > 0.0f ? v : 0.0f; }    // std::max<float>(0, v)
 
 // Every operation in the reference order (per output unit: bias, then inputs
-// ascending; layer 3 sums its inputs ascending). Layer 2's output units run four
-// at a time as independent chains, each still in reference order.
+// ascending; layer 3 sums its inputs ascending). Layer 2's output units run
+// WIDE_CHAINS at a time as independent chains, each still in reference order.
+#ifndef TA3B_WIDE_CHAINS
+#define TA3B_WIDE_CHAINS 4
+#endif
+constexpr int WIDE_CHAINS = TA3B_WIDE_CHAINS;
+static_assert(WH % WIDE_CHAINS == 0, "chains divide the layer");
 template <class WF>
 TA3B_HD float wide_forward(float const (&in)[NIN], WF const& w) {
     float h1[WH];
@@ -252,45 +257,37 @@ TA3B_HD float wide_forward(float const (&in)[NIN], WF const& w) {
     }
     float out = w(WIDE_B3);
 #pragma unroll 1
-    for (int o = 0; o < WH; o += 4) {
-        float a = w(WIDE_B2 + o), b = w(WIDE_B2 + o + 1), c = w(WIDE_B2 + o + 2), d = w(WIDE_B2 + o + 3);
+    for (int o = 0; o < WH; o += WIDE_CHAINS) {
+        float acc[WIDE_CHAINS];
+#pragma unroll
+        for (int k = 0; k < WIDE_CHAINS; ++k) acc[k] = w(WIDE_B2 + o + k);
         int const r = WIDE_W2 + o * WH;
         if (WF::VEC4) {
             // 16-byte loads of four consecutive weights of each row; the sums keep the reference order
 #pragma unroll
             for (int i = 0; i < WH; i += 4) {
-                auto const qa = w.v4(r + i), qb = w.v4(r + WH + i), qc = w.v4(r + 2 * WH + i),
-                           qd = w.v4(r + 3 * WH + i);
-                a = f_add(a, f_mul(h1[i], qa.x));
-                b = f_add(b, f_mul(h1[i], qb.x));
-                c = f_add(c, f_mul(h1[i], qc.x));
-                d = f_add(d, f_mul(h1[i], qd.x));
-                a = f_add(a, f_mul(h1[i + 1], qa.y));
-                b = f_add(b, f_mul(h1[i + 1], qb.y));
-                c = f_add(c, f_mul(h1[i + 1], qc.y));
-                d = f_add(d, f_mul(h1[i + 1], qd.y));
-                a = f_add(a, f_mul(h1[i + 2], qa.z));
-                b = f_add(b, f_mul(h1[i + 2], qb.z));
-                c = f_add(c, f_mul(h1[i + 2], qc.z));
-                d = f_add(d, f_mul(h1[i + 2], qd.z));
-                a = f_add(a, f_mul(h1[i + 3], qa.w));
-                b = f_add(b, f_mul(h1[i + 3], qb.w));
-                c = f_add(c, f_mul(h1[i + 3], qc.w));
-                d = f_add(d, f_mul(h1[i + 3], qd.w));
+                float q[WIDE_CHAINS][4];
+#pragma unroll
+                for (int k = 0; k < WIDE_CHAINS; ++k) {
+                    auto const v = w.v4(r + k * WH + i);
+                    q[k][0] = v.x;
+                    q[k][1] = v.y;
+                    q[k][2] = v.z;
+                    q[k][3] = v.w;
+                }
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+#pragma unroll
+                    for (int k = 0; k < WIDE_CHAINS; ++k) acc[k] = f_add(acc[k], f_mul(h1[i + j], q[k][j]));
             }
         } else {
 #pragma unroll
-            for (int i = 0; i < WH; ++i) {
-                a = f_add(a, f_mul(h1[i], w(r + i)));
-                b = f_add(b, f_mul(h1[i], w(r + WH + i)));
-                c = f_add(c, f_mul(h1[i], w(r + 2 * WH + i)));
-                d = f_add(d, f_mul(h1[i], w(r + 3 * WH + i)));
-            }
+            for (int i = 0; i < WH; ++i)
+#pragma unroll
+                for (int k = 0; k < WIDE_CHAINS; ++k) acc[k] = f_add(acc[k], f_mul(h1[i], w(r + k * WH + i)));
         }
-        out = f_add(out, f_mul(relu(a), w(WIDE_W3 + o)));
-        out = f_add(out, f_mul(relu(b), w(WIDE_W3 + o + 1)));
-        out = f_add(out, f_mul(relu(c), w(WIDE_W3 + o + 2)));
-        out = f_add(out, f_mul(relu(d), w(WIDE_W3 + o + 3)));
+#pragma unroll
+        for (int k = 0; k < WIDE_CHAINS; ++k) out = f_add(out, f_mul(relu(acc[k]), w(WIDE_W3 + o + k)));
     }
     return out;
 }
