@@ -39,6 +39,7 @@ enum {
     TA3B_ERR_CUDA = -2,    /* a CUDA runtime call failed (message has the CUDA error string) */
     TA3B_ERR_NODEV = -3,   /* no usable sm_100 device */
     TA3B_ERR_DEVICE = -4,  /* the kernel reported an error status */
+    TA3B_ERR_TIMEOUT = -5, /* the launch exceeded the context's time budget (ta3b_set_time_budget) */
 };
 
 typedef struct ta3b_ctx ta3b_ctx;
@@ -59,6 +60,13 @@ void ta3b_destroy(ta3b_ctx* ctx);
 
 /* Message of the last failure on this context (or of ta3b_create when ctx is NULL). */
 const char* ta3b_last_error(const ta3b_ctx* ctx);
+
+/* Per-launch time budget for this context's evaluations (0 = none, the default).
+ * Every warp compares the GPU's global timer with its launch start after each
+ * move; past the budget it stops (no new game, no further move) and the call
+ * returns TA3B_ERR_TIMEOUT, with incomplete results. The context stays usable.
+ * No reference counterpart (the reference has no device-side limit). */
+int ta3b_set_time_budget(ta3b_ctx* ctx, double seconds);
 
 /* Batched evaluation with host buffers: num_models models, each played on the
  * SAME num_games seeds. weights is model-major, num_models * num_params floats

@@ -194,3 +194,20 @@ def test_generation_graph_replays_match_direct_calls(ev):
         s2, p2, l2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
         assert sc.tobytes() == s2.tobytes() and np.array_equal(pc, p2) and np.array_equal(lc, l2)
         assert (ec > 0).all()
+
+
+def test_time_budget_stops_the_launch_and_keeps_the_context(ev):
+    """A budget far below the batch's run time ends the launch early with
+    TA3B_ERR_TIMEOUT (no fault); without a budget the same context then scores
+    the batch exactly as before."""
+    from tetris_ai3_b200 import EvaluatorError, workload
+    b = workload.generation_batch(islands=2, pop=20, games=20, max_moves=2000, seed=3)
+    ref = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    ev.set_time_budget(1e-4)
+    with pytest.raises(EvaluatorError, match="time budget"):
+        ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    ev.set_time_budget(0)
+    again = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    assert all(x.tobytes() == y.tobytes() for x, y in zip(ref, again))
+    with pytest.raises(EvaluatorError):
+        ev.set_time_budget(-1.0)

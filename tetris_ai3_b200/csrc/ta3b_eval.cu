@@ -351,6 +351,7 @@ struct Params {
     uint32_t* board_out;
     uint32_t* scratch;                 // [0] sim ticket, [1] error status
     unsigned long long* timing;        // optional: per sim [start, end] global timer (ns)
+    unsigned long long budget_ns;      // 0, or the launch's time budget: past it warps stop and set status bit 2
     uint32_t num_games, models_per_island, max_moves, total_sims;
 };
 
@@ -678,7 +679,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     Luts const lut{s_lut.fast, s_lut.move};
     int const lane = int(threadIdx.x & 31u);
     WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
+    // time budget, measured from this warp's start (the persistent grid starts every warp at launch)
+    unsigned long long t_start = 0;
+    if (p.budget_ns) {
+        if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
+        t_start = __shfl_sync(FULL_MASK, t_start, 0);
+    }
+    bool out_of_time = false;
     for (;;) {
+        if (out_of_time) break;
         uint32_t sim = 0;
         if (lane == 0) sim = atomicAdd(&p.scratch[0], 1u);
         sim = __shfl_sync(FULL_MASK, sim, 0);
@@ -722,6 +731,16 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             ++moves;
             __syncwarp();
             if (ws.eng.over == 2) break;
+            if (p.budget_ns) {
+                unsigned long long now = 0;
+                if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+                now = __shfl_sync(FULL_MASK, now, 0);
+                if (now - t_start > p.budget_ns) {
+                    if (lane == 0) atomicOr(&p.scratch[1], 2u);
+                    out_of_time = true;
+                    break;
+                }
+            }
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
         if (lane == 0) {
@@ -836,6 +855,7 @@ struct ta3b_ctx {
     size_t cap_timing = 0;
     float* d_wpad = nullptr;          // widened models in their padded device layout
     size_t cap_wpad = 0;
+    unsigned long long budget_ns = 0; // per-launch time budget (0 = none)
     int wide_variant = -1;            // widened-network kernel, set up on first use
     uint32_t wide_warps = 0, wide_grid = 0;
     std::string err;
@@ -909,7 +929,9 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, bool wide = false)
     uint32_t const need_blocks = (prm.total_sims + warps - 1) / warps;
     uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
     KernelFn const fn = wide ? kWideVariants[ctx->wide_variant].fn : kVariants[ctx->variant].fn;
-    fn<<<grid, warps * 32, warps * sizeof(WarpShared), st>>>(prm);
+    Params p2 = prm;
+    p2.budget_ns = ctx->budget_ns;
+    fn<<<grid, warps * 32, warps * sizeof(WarpShared), st>>>(p2);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     return TA3B_OK;
 }
@@ -919,7 +941,9 @@ int read_status(ta3b_ctx* ctx) {
     TA3B_CUDA(ctx, cudaMemcpyAsync(&status, ctx->d_scratch + 1, sizeof status, cudaMemcpyDeviceToHost, ctx->stream),
               "read status");
     TA3B_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "kernel run");
-    if (status) return fail(ctx, TA3B_ERR_DEVICE, "kernel reported status " + std::to_string(status));
+    if (status & 1u) return fail(ctx, TA3B_ERR_DEVICE, "kernel reported status " + std::to_string(status));
+    if (status & 2u)
+        return fail(ctx, TA3B_ERR_TIMEOUT, "time budget exceeded: the launch stopped early, results are incomplete");
     return TA3B_OK;
 }
 
@@ -1229,6 +1253,13 @@ int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_bloc
     if (variant < 0 || variant >= kNumVariants) return TA3B_ERR_ARG;
     if (warps_per_block) *warps_per_block = kVariants[variant].warps;
     if (min_blocks_per_sm) *min_blocks_per_sm = kVariants[variant].min_blocks;
+    return TA3B_OK;
+}
+
+int ta3b_set_time_budget(ta3b_ctx* ctx, double seconds) {
+    if (!ctx) return TA3B_ERR_ARG;
+    if (!(seconds >= 0.0) || seconds > 1.0e6) return fail(ctx, TA3B_ERR_ARG, "time budget must be in [0, 1e6] s");
+    ctx->budget_ns = static_cast<unsigned long long>(seconds * 1.0e9);
     return TA3B_OK;
 }
 

@@ -31,7 +31,7 @@ _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
            "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
-           "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc"]
+           "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc", "ta3b_set_time_budget"]
 
 
 class EvaluatorError(RuntimeError):
@@ -67,6 +67,7 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_num_variants.argtypes = []
     lib.ta3b_variant_info.argtypes = [C.c_int, vp, vp]
     lib.ta3b_select_variant.argtypes = [vp, C.c_int]
+    lib.ta3b_set_time_budget.argtypes = [vp, C.c_double]
     lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
     lib.ta3b_eval_device_noalloc.argtypes = [vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp,
                                              C.POINTER(C.c_char_p)]
@@ -197,6 +198,10 @@ class ModelEvaluator:
         self._check(self._lib.ta3b_eval_device(self._ctx, ptr(weights), islands, models // islands, nparams,
                                                ptr(seeds), games, max_moves, ptr(score), ptr(pieces), ptr(lines),
                                                ptr(evals), st))
+
+    def set_time_budget(self, seconds: float):
+        """Per-launch time budget (0 = none): past it the call raises with an incomplete batch."""
+        self._check(self._lib.ta3b_set_time_budget(self._ctx, float(seconds)))
 
     def select_variant(self, variant: int):
         self._check(self._lib.ta3b_select_variant(self._ctx, variant))
