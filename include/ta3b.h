@@ -65,6 +65,8 @@ const char* ta3b_last_error(const ta3b_ctx* ctx);
  * Every warp compares the GPU's global timer with its launch start after each
  * move; past the budget it stops (no new game, no further move) and the call
  * returns TA3B_ERR_TIMEOUT, with incomplete results. The context stays usable.
+ * While a budget is set, launches use a fixed launch shape (the checking
+ * flavour of the kernel), not the one chosen by ta3b_select_variant.
  * No reference counterpart (the reference has no device-side limit). */
 int ta3b_set_time_budget(ta3b_ctx* ctx, double seconds);
 

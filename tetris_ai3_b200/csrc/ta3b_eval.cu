@@ -330,7 +330,7 @@ struct alignas(16) WarpShared {
     uint32_t rec[33][REC_WORDS];      // kept frontier records (rank -> record); [32] = committed board
     float wfull[NPARAMS + 3];         // the v11 model's weights (full path, record partial sums)
     float const* wglobal;              // the widened model's weights (global memory)
-    uint32_t pad_[2];
+    unsigned long long t_start;        // the launch's start on this warp (time budget)
     Engine eng;                        // the committed game
     Stats st;
     uint32_t seg_off[65];              // a level's candidate segments (parent rank, child list)
@@ -666,8 +666,10 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     return mv;
 }
 
-// WIDE: the widened 10 -> 64 -> 64 -> 1 network (4,929 weights per model) instead of v11
-template <int WARPS, int MINB, bool WIDE = false>
+// WIDE: the widened 10 -> 64 -> 64 -> 1 network (4,929 weights per model) instead of v11.
+// BUDGET: the flavour that checks the launch's time budget after every move (a separate
+// instantiation: the check's registers would otherwise cost the ordinary kernels spills).
+template <int WARPS, int MINB, bool WIDE = false, bool BUDGET = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
@@ -679,15 +681,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     Luts const lut{s_lut.fast, s_lut.move};
     int const lane = int(threadIdx.x & 31u);
     WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
-    // time budget, measured from this warp's start (the persistent grid starts every warp at launch)
-    unsigned long long t_start = 0;
-    if (p.budget_ns) {
-        if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_start));
-        t_start = __shfl_sync(FULL_MASK, t_start, 0);
-    }
-    bool out_of_time = false;
+    // time budget, measured from this warp's start (the persistent grid starts every warp at launch);
+    // kept in shared memory so it costs no register in the move loop
+    if (BUDGET && lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ws.t_start));
     for (;;) {
-        if (out_of_time) break;
         uint32_t sim = 0;
         if (lane == 0) sim = atomicAdd(&p.scratch[0], 1u);
         sim = __shfl_sync(FULL_MASK, sim, 0);
@@ -731,15 +728,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             ++moves;
             __syncwarp();
             if (ws.eng.over == 2) break;
-            if (p.budget_ns) {
-                unsigned long long now = 0;
-                if (lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
-                now = __shfl_sync(FULL_MASK, now, 0);
-                if (now - t_start > p.budget_ns) {
-                    if (lane == 0) atomicOr(&p.scratch[1], 2u);
-                    out_of_time = true;
-                    break;
+            if (BUDGET) {                                          // over = 3: out of time, stop here
+                if (lane == 0) {
+                    unsigned long long now;
+                    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+                    if (now - ws.t_start > p.budget_ns) {
+                        atomicOr(&p.scratch[1], 2u);
+                        ws.eng.over = 3;
+                    }
                 }
+                __syncwarp();
+                if (ws.eng.over == 3) break;
             }
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
@@ -758,6 +757,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             }
         }
         __syncwarp();
+        if (BUDGET && ws.eng.over == 3) break;                   // out of time: take no further sim
     }
 }
 
@@ -819,6 +819,9 @@ Variant const kWideVariants[] = {
     {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
 };
 constexpr int kDefaultWideVariant = 0;
+// the budget-checking flavours (shapes where the extra check spills nothing)
+Variant const kBudgetV11 = {eval_kernel<4, 3, false, true>, 4, 3};
+Variant const kBudgetWide = {eval_kernel<4, 2, true, true>, 4, 2};
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
@@ -857,6 +860,7 @@ struct ta3b_ctx {
     size_t cap_wpad = 0;
     unsigned long long budget_ns = 0; // per-launch time budget (0 = none)
     int wide_variant = -1;            // widened-network kernel, set up on first use
+    uint32_t budget_grid[2] = {0, 0};  // budget flavours (v11, widened), set up on first use
     uint32_t wide_warps = 0, wide_grid = 0;
     std::string err;
 };
@@ -919,16 +923,35 @@ int setup_wide(ta3b_ctx* ctx) {
     return TA3B_OK;
 }
 
+int setup_budget(ta3b_ctx* ctx, bool wide) {
+    if (ctx->budget_grid[wide]) return TA3B_OK;
+    Variant const& v = wide ? kBudgetWide : kBudgetV11;
+    size_t const dyn = v.warps * sizeof(WarpShared);
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                        cudaSharedmemCarveoutMaxShared), "smem carveout");
+    int per_sm = 0;
+    TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
+    if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "budget kernel does not fit on an SM");
+    ctx->budget_grid[wide] = ctx->sms * uint32_t(per_sm);
+    return TA3B_OK;
+}
+
 int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, bool wide = false) {
     if (prm.total_sims == 0) return TA3B_OK;
     if (wide)
         if (int rc = setup_wide(ctx)) return rc;
+    bool const budget = ctx->budget_ns != 0;
+    if (budget)
+        if (int rc = setup_budget(ctx, wide)) return rc;
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, 2 * sizeof(uint32_t), st), "reset work queue");
-    uint32_t const warps = wide ? ctx->wide_warps : ctx->warps_per_block;
-    uint32_t const max_grid = wide ? ctx->wide_grid : ctx->grid;
+    // with a time budget the budget-checking flavour runs (its own fixed launch shape)
+    Variant const* bv = budget ? (wide ? &kBudgetWide : &kBudgetV11) : nullptr;
+    uint32_t const warps = bv ? bv->warps : wide ? ctx->wide_warps : ctx->warps_per_block;
+    uint32_t const max_grid = bv ? ctx->budget_grid[wide] : wide ? ctx->wide_grid : ctx->grid;
     uint32_t const need_blocks = (prm.total_sims + warps - 1) / warps;
     uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
-    KernelFn const fn = wide ? kWideVariants[ctx->wide_variant].fn : kVariants[ctx->variant].fn;
+    KernelFn const fn = bv ? bv->fn : wide ? kWideVariants[ctx->wide_variant].fn : kVariants[ctx->variant].fn;
     Params p2 = prm;
     p2.budget_ns = ctx->budget_ns;
     fn<<<grid, warps * 32, warps * sizeof(WarpShared), st>>>(p2);
