@@ -29,3 +29,32 @@ def test_trainer_on_gpu_equals_trainer_on_oracle(host, oracle):
         assert np.array_equal(gpu.island_mean(i), cpu.island_mean(i))
     sg, sc = gpu.stats(), cpu.stats()
     assert sg["pieces"] == sc["pieces"] and sg["sims"] == sc["sims"] and sg["best_fitness"] == sc["best_fitness"]
+
+
+def test_widened_trainer_on_gpu_equals_trainer_on_oracle(host, oracle):
+    """The trainer with the widened network (sep-CMA-ES, 4,929 parameters) on the
+    GPU's widened kernel and on the oracle's widened restatement: same champions."""
+    import ctypes as C
+    from conftest import ptr
+    cfg = dict(islands=2, population=6, gens_per_iteration=2, iterations_per_cycle=2, games=2, max_moves=60,
+               algo=host.SEP, num_params=4929, sigma0=0.1)
+
+    def score(w, seeds, mm):
+        w = np.ascontiguousarray(w, np.float32)
+        s = np.ascontiguousarray(seeds, np.uint64)
+        n = len(w) * len(s)
+        sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+        ev = C.c_uint64()
+        oracle.ta3o_eval_net_mt(ptr(w), 64, 64, len(w), ptr(s), len(s), mm, 8, ptr(sc), ptr(pc), ptr(lc),
+                                C.byref(ev))
+        return sc.reshape(len(w), -1), pc.reshape(len(w), -1)
+
+    gpu = host.Trainer(host.default_config(**cfg))
+    cpu = host.Trainer(host.default_config(**cfg), score=score)
+    gpu.run(2)
+    cpu.run(2)
+    for i in range(cfg["islands"]):
+        xg, fg = gpu.champion(i)
+        xc, fc = cpu.champion(i)
+        assert fg == fc and np.array_equal(xg, xc)
+    assert gpu.stats()["pieces"] == cpu.stats()["pieces"]

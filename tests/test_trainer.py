@@ -203,3 +203,21 @@ def test_surrogate_window_limits_the_training_set(host):
     # retrains at generations 6 and 8: the two generations before the held-out one
     assert seen[0] == 2 * per_gen
     assert seen[1] == per_gen + c.islands * (6 + 2)
+
+
+def test_sep_cmaes_trains_the_widened_parameter_vector(host):
+    """4,929 parameters (the widened 10-64-64-1 network): sep-CMA-ES, O(n) per sample."""
+    target = np.linspace(-0.5, 0.5, 4929)
+
+    def score(w, seeds, mm):
+        return np.repeat(-((w.astype(np.float64) - target) ** 2).sum(1, keepdims=True), len(seeds), 1)
+
+    c = small(host, algo=host.SEP, num_params=4929, sigma0=0.05, population=12)
+    t = host.Trainer(c, score=score)
+    t2 = host.Trainer(c, score=score)
+    t.run(2)
+    t2.run(2)
+    assert t.calls == [(c.islands * c.population, c.games, c.max_moves)] * (1 + 2 * c.gens_per_iteration)
+    x, f = t.champion(0)
+    assert x.shape == (4929,) and np.isfinite(f) and np.isfinite(t.island_mean(0)).all()
+    assert np.array_equal(t.island_mean(1), t2.island_mean(1))        # deterministic at n = 4929
