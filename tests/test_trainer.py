@@ -221,3 +221,13 @@ def test_sep_cmaes_trains_the_widened_parameter_vector(host):
     x, f = t.champion(0)
     assert x.shape == (4929,) and np.isfinite(f) and np.isfinite(t.island_mean(0)).all()
     assert np.array_equal(t.island_mean(1), t2.island_mean(1))        # deterministic at n = 4929
+
+
+def test_corrupt_champ_files_are_rejected(host, tmp_path):
+    p = tmp_path / "bad.champ"
+    p.write_bytes(np.uint64(10 ** 12).tobytes() + np.zeros(4).tobytes())      # count beyond the file
+    with pytest.raises(OSError):
+        host.read_champ(str(p))
+    p.write_bytes(b"\x01\x02")
+    with pytest.raises(OSError):
+        host.read_champ(str(p))

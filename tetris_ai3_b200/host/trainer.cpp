@@ -605,9 +605,13 @@ int ta3t_write_champ(const char* path, const double* x, uint64_t n) {
 }
 
 uint64_t ta3t_read_champ(const char* path, double* x_out, uint64_t cap) {
-    std::ifstream f(path ? path : "", std::ios::binary);
+    std::ifstream f(path ? path : "", std::ios::binary | std::ios::ate);
+    if (!f) return 0;
+    auto const size = uint64_t(f.tellg());
+    f.seekg(0);
     uint64_t n = 0;
-    if (!f || !f.read(reinterpret_cast<char*>(&n), sizeof n)) return 0;
+    if (!f.read(reinterpret_cast<char*>(&n), sizeof n)) return 0;
+    if (size < sizeof n || n != (size - sizeof n) / sizeof(double)) return 0;   // count must match the file
     std::vector<double> v(n);
     if (!f.read(reinterpret_cast<char*>(v.data()), std::streamsize(n * sizeof(double)))) return 0;
     if (x_out) std::memcpy(x_out, v.data(), std::min(n, cap) * sizeof(double));
