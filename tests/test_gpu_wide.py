@@ -64,3 +64,52 @@ def test_v11_and_wide_share_a_context(ev):
     v = ev.eval(b1.weights, 1, b1.seeds[0][:2], 60)
     a2 = ev.eval(w[:2], 2, seeds[:2], 60)
     assert a.tobytes() == a2.tobytes() and v.shape == (2,)
+
+
+def _oracle_net(oracle, w, seeds, max_moves):
+    n = w.shape[0] * seeds.size
+    osc, opc, olc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    ev_total = C.c_uint64()
+    oracle.ta3o_eval_net_mt(ptr(w), 64, 64, w.shape[0], ptr(seeds), seeds.size, max_moves, 8, ptr(osc), ptr(opc),
+                            ptr(olc), C.byref(ev_total))
+    return osc, opc, olc
+
+
+def _variant_models():
+    """Widened models that exercise the kernel's zero-term skipping from both sides:
+    heavily sparse hidden layers (negative first-layer biases), exact zero weights,
+    and models where skipping is not allowed (a -0 bias; the kernel then runs every term)."""
+    from tetris_ai3_b200 import workload
+    b = workload.wide_batch(islands=1, pop=6, games=3, max_moves=120, seed=11)
+    w = b.weights.copy()
+    assert w.shape[1] == workload.NUM_PARAMS_WIDE
+    w1, b1, w2, b2 = slice(0, 640), slice(640, 704), slice(704, 4800), slice(4800, 4864)   # [out][in] then biases
+    w[0, b1] = -0.75                              # most first-layer units are zero in every lane
+    w[1, b1] = np.float32(-0.0)                   # -0 biases: skipping disabled
+    w[2, b2] = np.float32(-0.0)
+    w[2, b1] = 0.25
+    w[3, w2.start:w2.stop:3] = 0.0                # exact zero weights in layer 2
+    w[4, w1.start:w1.stop:2] = 0.0                # and in layer 1
+    w[5, b1] = np.linspace(-1.0, 1.0, 64, dtype=np.float32)
+    return w, np.ascontiguousarray(b.seeds[0]), b.max_moves
+
+
+def test_wide_zero_skipping_is_exact(ev, oracle):
+    w, seeds, cap = _variant_models()
+    sc, pc, lc = ev.eval_full(w, w.shape[0], seeds, cap)
+    osc, opc, olc = _oracle_net(oracle, w, seeds, cap)
+    assert sc.tobytes() == osc.tobytes()
+    assert np.array_equal(pc, opc) and np.array_equal(lc, olc)
+
+
+def test_wide_device_entry_matches_host_entry(ev):
+    import torch
+    w, seeds, cap = _variant_models()
+    host = ev.eval(w, w.shape[0], seeds, cap)
+    dev = torch.device("cuda", 0)
+    dw = torch.from_numpy(w).to(dev)
+    ds = torch.from_numpy(seeds.view(np.int64).reshape(1, -1)).to(dev)
+    score = torch.zeros(w.shape[0] * seeds.size, dtype=torch.float32, device=dev)
+    ev.eval_device(dw, ds, cap, score)
+    torch.cuda.synchronize()
+    assert score.cpu().numpy().tobytes() == host.tobytes()

@@ -230,72 +230,26 @@ constexpr int WH = 64;
 constexpr int WIDE_B1 = NIN * WH, WIDE_W2 = WIDE_B1 + WH, WIDE_B2 = WIDE_W2 + WH * WH, WIDE_W3 = WIDE_B2 + WH,
               WIDE_B3 = WIDE_W3 + WH, NPARAMS_WIDE = WIDE_B3 + 1;
 static_assert(NPARAMS_WIDE == 4929, "10 -> 64 -> 64 -> 1");
-// device copies of widened models are padded to a 16-byte multiple, so layer 2's rows
-// (which start at WIDE_W2 = 768 floats) can be read with 16-byte loads
-constexpr int WIDE_STRIDE = 4932;
-static_assert(WIDE_STRIDE % 4 == 0 && WIDE_STRIDE >= NPARAMS_WIDE && WIDE_W2 % 4 == 0 && WH % 4 == 0, "alignment");
+// Device copy of a widened model (WIDE_STRIDE floats, 16-byte aligned): the same
+// offsets, but layers 1 and 2 transposed to [in][out], so one input's weights to all
+// 64 units are contiguous; the word after the last bias is WIDE_SKIP (below).
+constexpr int WIDE_W1T = 0, WIDE_W2T = WIDE_W2, WIDE_SKIP = NPARAMS_WIDE, WIDE_STRIDE = 4932;
+static_assert(WIDE_STRIDE % 4 == 0 && WIDE_STRIDE > WIDE_SKIP && WIDE_B1 % 4 == 0 && WIDE_W2 % 4 == 0 &&
+                  WIDE_B2 % 4 == 0 && WIDE_W3 % 4 == 0 && WH % 4 == 0, "16-byte aligned blocks");
+// Device-layout index of parameter j of a widened model (reference order).
+TA3B_HD int wide_device_index(int j) {
+    if (j < WIDE_B1) return WIDE_W1T + (j % NIN) * WH + j / NIN;
+    if (j >= WIDE_W2 && j < WIDE_B2) return WIDE_W2T + ((j - WIDE_W2) % WH) * WH + (j - WIDE_W2) / WH;
+    return j;
+}
+TA3B_HD bool wide_is_bias(int j) {
+    return (j >= WIDE_B1 && j < WIDE_W2) || (j >= WIDE_B2 && j < WIDE_W3) || j == WIDE_B3;
+}
 
 TA3B_HD float relu(float v) { return v > 0.0f ? v : 0.0f; }    // std::max<float>(0, v)
 
-// Every operation in the reference order (per output unit: bias, then inputs
-// ascending; layer 3 sums its inputs ascending). Layer 2's output units run
-// WIDE_CHAINS at a time as independent chains, each still in reference order.
-#ifndef TA3B_WIDE_CHAINS
-#define TA3B_WIDE_CHAINS 4
-#endif
-constexpr int WIDE_CHAINS = TA3B_WIDE_CHAINS;
-static_assert(WH % WIDE_CHAINS == 0, "chains divide the layer");
-template <class WF>
-TA3B_HD float wide_forward(float const (&in)[NIN], WF const& w) {
-    float h1[WH];
-#pragma unroll
-    for (int o = 0; o < WH; ++o) {
-        float v = w(WIDE_B1 + o);
-#pragma unroll
-        for (int i = 0; i < NIN; ++i) v = f_add(v, f_mul(in[i], w(o * NIN + i)));
-        h1[o] = relu(v);
-    }
-    float out = w(WIDE_B3);
-#pragma unroll 1
-    for (int o = 0; o < WH; o += WIDE_CHAINS) {
-        float acc[WIDE_CHAINS];
-#pragma unroll
-        for (int k = 0; k < WIDE_CHAINS; ++k) acc[k] = w(WIDE_B2 + o + k);
-        int const r = WIDE_W2 + o * WH;
-        if (WF::VEC4) {
-            // 16-byte loads of four consecutive weights of each row; the sums keep the reference order
-#pragma unroll
-            for (int i = 0; i < WH; i += 4) {
-                float q[WIDE_CHAINS][4];
-#pragma unroll
-                for (int k = 0; k < WIDE_CHAINS; ++k) {
-                    auto const v = w.v4(r + k * WH + i);
-                    q[k][0] = v.x;
-                    q[k][1] = v.y;
-                    q[k][2] = v.z;
-                    q[k][3] = v.w;
-                }
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-#pragma unroll
-                    for (int k = 0; k < WIDE_CHAINS; ++k) acc[k] = f_add(acc[k], f_mul(h1[i + j], q[k][j]));
-            }
-        } else {
-#pragma unroll
-            for (int i = 0; i < WH; ++i)
-#pragma unroll
-                for (int k = 0; k < WIDE_CHAINS; ++k) acc[k] = f_add(acc[k], f_mul(h1[i], w(r + k * WH + i)));
-        }
-#pragma unroll
-        for (int k = 0; k < WIDE_CHAINS; ++k) out = f_add(out, f_mul(relu(acc[k]), w(WIDE_W3 + o + k)));
-    }
-    return out;
-}
-
-// model_v11.hpp:63-91 inputs, then the widened network
-template <class WF>
-TA3B_HD float value_full_wide(uint32_t clear_bits, BoardInts const& bi, bool held_i, WF const& w) {
-    float in[NIN];
+// model_v11.hpp:63-91 inputs of the widened network
+TA3B_HD void wide_inputs(uint32_t clear_bits, BoardInts const& bi, bool held_i, float (&in)[NIN]) {
 #pragma unroll
     for (int k = 0; k < 4; ++k) in[k] = f_mul(float((clear_bits >> (8 * k)) & 0xFFu), 0.25f);
     in[4] = div_exact(bi.surf_sq > 0 ? f_sqrt(float(bi.surf_sq)) : 0.0f, 100.0f, R100);
@@ -304,7 +258,6 @@ TA3B_HD float value_full_wide(uint32_t clear_bits, BoardInts const& bi, bool hel
     in[7] = float(bi.max_height);
     in[8] = held_i ? 1.0f : 0.0f;
     in[9] = div_exact(float(bi.wells), 5.0f, R5);
-    return wide_forward(in, w);
 }
 
 // --------------------------------------------------------- packed FP32x2 ---
@@ -707,24 +660,23 @@ TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& 
     return defer ? FAST_DEFER : FAST_OK;
 }
 
-// The fast path for the widened network: the same features, the parent's clear
-// counts as the first four inputs (a fast candidate clears no row).
-template <class WF>
-TA3B_HD int fast_eval_wide(RecView const& r, uint32_t clear_bits, PlaceFast pf, bool held_i, WF const& w,
-                           float& value) {
+// The fast path's inputs of the widened network: the same features, the parent's
+// clear counts as the first four inputs (a fast candidate clears no row). Returns
+// true when the candidate must take the full path instead (inputs then all zero).
+TA3B_HD bool fast_wide_inputs(RecView const& r, uint32_t clear_bits, PlaceFast pf, bool held_i, float (&in)[NIN]) {
     FastFeat ff;
     bool const defer = fast_features(r, pf, ff);
-    float in[NIN];
+    BoardInts bi;
+    bi.surf_sq = ff.surf;
+    bi.holes = ff.holes;
+    bi.hole_depths = ff.hd;
+    bi.max_height = ff.maxh;
+    bi.wells = ff.wells;
+    wide_inputs(clear_bits, bi, held_i, in);
+    if (defer)
 #pragma unroll
-    for (int k = 0; k < 4; ++k) in[k] = f_mul(float((clear_bits >> (8 * k)) & 0xFFu), 0.25f);
-    in[4] = div_exact(ff.surf > 0 ? f_sqrt(float(ff.surf)) : 0.0f, 100.0f, R100);
-    in[5] = div_exact(float(ff.holes), 20.0f, R20);
-    in[6] = div_exact(float(ff.hd), 200.0f, R200);
-    in[7] = float(ff.maxh);
-    in[8] = held_i ? 1.0f : 0.0f;
-    in[9] = div_exact(float(ff.wells), 5.0f, R5);
-    value = defer ? 0.0f : wide_forward(in, w);
-    return defer ? FAST_DEFER : FAST_OK;
+        for (int i = 0; i < NIN; ++i) in[i] = 0.0f;
+    return defer;
 }
 
 } // namespace ta3b

@@ -207,14 +207,6 @@ struct GlobalW {
     float const* p;
     __device__ __forceinline__ float operator()(int i) const { return __ldg(p + i); }
 };
-// a widened model's padded device copy (16-byte aligned, WIDE_STRIDE floats per model)
-struct WideW {
-    static constexpr bool VEC4 = true;
-    float const* p;
-    __device__ __forceinline__ float operator()(int i) const { return __ldg(p + i); }
-    __device__ __forceinline__ float4 v4(int i) const { return __ldg(reinterpret_cast<float4 const*>(p + i)); }
-};
-
 __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uint32_t (&b)[W]) {
     uint4 const q0 = *reinterpret_cast<uint4 const*>(src);
     uint4 const q1 = *reinterpret_cast<uint4 const*>(src + 4);
@@ -248,16 +240,112 @@ __device__ __forceinline__ int fast_candidate(uint32_t const* __restrict__ rec, 
     return fast_eval<MLP>(r, pf, held_i, fw, v, dbg);
 }
 
-// fast path of the widened network: the same record words, the weights from global memory
+// ------------------------------------------------ widened network (device) ---
+// One lane = one candidate; the warp's lanes run the network together so that a
+// term can be left out when its input is exactly zero in every lane. That is
+// exact: x + (±0 * w) == x for finite w and every x but -0, and a sum that starts
+// from a bias other than -0 is never -0 (under round-to-nearest a sum is -0 only
+// for (-0) + (-0)). repack_wide_kernel sets WIDE_SKIP for models whose weights
+// are all finite and whose biases are not -0; every other model runs every term.
+// Each unit's sum keeps the reference order (utility.hpp:30-46: bias, then the
+// inputs ascending), only without the zero terms. Lanes without a candidate pass
+// zero inputs. hb: this warp's hidden-unit buffer, [unit / 4][lane] float4.
+struct WideIn {
+    float v[NIN];
+};
+constexpr int WIDE_HB_FLOAT4 = WH / 4 * WARP;          // per warp: 64 units x 32 lanes (8 KB)
+
+__device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w, float4* __restrict__ hb, int lane) {
+    uint32_t const skip = __ldg(reinterpret_cast<uint32_t const*>(w) + WIDE_SKIP);
+    float a[WH];
+#pragma unroll
+    for (int o = 0; o < WH; o += 4) {
+        float4 const b = __ldg(reinterpret_cast<float4 const*>(w + WIDE_B1 + o));
+        a[o] = b.x; a[o + 1] = b.y; a[o + 2] = b.z; a[o + 3] = b.w;
+    }
+    // layer 1, one input at a time over all 64 units (inputs that are zero in every lane skipped)
+    uint32_t inz = 0;
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) inz |= in.v[i] != 0.0f ? 1u << i : 0u;
+    inz = skip ? __reduce_or_sync(FULL_MASK, inz) : (1u << NIN) - 1u;
+#pragma unroll
+    for (int i = 0; i < NIN; ++i) {
+        if (!((inz >> i) & 1u)) continue;
+        float4 const* wr = reinterpret_cast<float4 const*>(w + WIDE_W1T + i * WH);
+        float const x = in.v[i];
+#pragma unroll
+        for (int o = 0; o < WH; o += 4) {
+            float4 const q = __ldg(wr + o / 4);
+            a[o] = f_add(a[o], f_mul(x, q.x));
+            a[o + 1] = f_add(a[o + 1], f_mul(x, q.y));
+            a[o + 2] = f_add(a[o + 2], f_mul(x, q.z));
+            a[o + 3] = f_add(a[o + 3], f_mul(x, q.w));
+        }
+    }
+    // ReLU into the buffer; nz = the units that are non-zero in some lane
+    uint32_t nz[2] = {0u, 0u};
+#pragma unroll
+    for (int o = 0; o < WH; o += 4) {
+        float4 const h = make_float4(relu(a[o]), relu(a[o + 1]), relu(a[o + 2]), relu(a[o + 3]));
+        hb[(o / 4) * WARP + lane] = h;
+        uint32_t const bits = (h.x != 0.0f ? 1u : 0u) | (h.y != 0.0f ? 2u : 0u) | (h.z != 0.0f ? 4u : 0u) |
+                              (h.w != 0.0f ? 8u : 0u);
+        nz[o >> 5] |= bits << (o & 31);
+    }
+    if (skip) {
+        nz[0] = __reduce_or_sync(FULL_MASK, nz[0]);
+        nz[1] = __reduce_or_sync(FULL_MASK, nz[1]);
+    } else {
+        nz[0] = nz[1] = ~0u;
+    }
+    // layer 2, one hidden unit at a time over all 64 outputs
+#pragma unroll
+    for (int o = 0; o < WH; o += 4) {
+        float4 const b = __ldg(reinterpret_cast<float4 const*>(w + WIDE_B2 + o));
+        a[o] = b.x; a[o + 1] = b.y; a[o + 2] = b.z; a[o + 3] = b.w;
+    }
+    float const* hs = reinterpret_cast<float const*>(hb) + 4 * lane;
+    uint64_t m = (uint64_t(nz[1]) << 32) | nz[0];
+    while (m) {
+        int const i = __ffsll(static_cast<long long>(m)) - 1;
+        m &= m - 1;
+        float const x = hs[(i >> 2) * (4 * WARP) + (i & 3)];
+        float4 const* wr = reinterpret_cast<float4 const*>(w + WIDE_W2T + i * WH);
+#pragma unroll
+        for (int o = 0; o < WH; o += 4) {
+            float4 const q = __ldg(wr + o / 4);
+            a[o] = f_add(a[o], f_mul(x, q.x));
+            a[o + 1] = f_add(a[o + 1], f_mul(x, q.y));
+            a[o + 2] = f_add(a[o + 2], f_mul(x, q.z));
+            a[o + 3] = f_add(a[o + 3], f_mul(x, q.w));
+        }
+    }
+    // layer 3: every term, ascending
+    float out = __ldg(w + WIDE_B3);
+#pragma unroll
+    for (int o = 0; o < WH; o += 4) {
+        float4 const q = __ldg(reinterpret_cast<float4 const*>(w + WIDE_W3 + o));
+        out = f_add(out, f_mul(relu(a[o]), q.x));
+        out = f_add(out, f_mul(relu(a[o + 1]), q.y));
+        out = f_add(out, f_mul(relu(a[o + 2]), q.z));
+        out = f_add(out, f_mul(relu(a[o + 3]), q.w));
+    }
+    return out;
+}
+
+// fast path of the widened network: the same record words; every lane of the warp calls it
 __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ rec, PlaceFast pf, bool held_i,
-                                                   float const* __restrict__ w, float& v) {
+                                                   float const* __restrict__ w, float4* hb, int lane, float& v) {
     RecView r;
     uint4 const q = *reinterpret_cast<uint4 const*>(rec + R_HD);
     r.hd = q.x; r.rc0 = q.y; r.rc1 = q.z; r.rc2 = q.w;
     r.tot = rec[R_TOT];
     span_of(rec, int((pf.m >> 27) & 0xFu), r.h4, r.hm4);
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
-    return fast_eval_wide(r, rec[R_CLEARS], pf, held_i, WideW{w}, v);
+    WideIn in;
+    bool const defer = fast_wide_inputs(r, rec[R_CLEARS], pf, held_i, in.v);
+    v = wide_value(in, w, hb, lane);
+    return defer ? FAST_DEFER : FAST_OK;
 }
 
 // stats_v4::advance (tetris_stats.hpp:19-23 with metrics.hpp:196-229)
@@ -381,7 +469,6 @@ struct Luts {
 
 // Full path for one queued candidate (segment << 8 | placement): its key, or 0 if illegal.
 // A legal candidate's key is never 0 (its low word is a positive position).
-template <bool WIDE>
 __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, uint32_t entry) {
     uint32_t const seg = entry >> 8, i = entry & 0xFFu;
     uint32_t const info = ws->seg_info[seg];
@@ -392,9 +479,23 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
     int cl = 0;
     if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return 0;
     BoardInts const bi = board_ints(nb);
-    float const v = WIDE ? value_full_wide(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, WideW{ws->wglobal})
-                         : value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
+    float const v = value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
     return candidate_key(leaf, v, info, i);
+}
+
+// The widened network's full path, first half: is the queued candidate legal,
+// and its inputs (all zero when it is not).
+__device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t entry, WideIn& in) {
+    uint32_t const seg = entry >> 8, i = entry & 0xFFu;
+    uint32_t const info = ws->seg_info[seg];
+    uint32_t const* rec = ws->rec[info & 63u];
+    uint32_t const mv = lut.move[(info >> 16) & 7u][i];
+    uint32_t b[W], nb[W];
+    load_board(rec + R_BOARD, b);
+    int cl = 0;
+    if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return false;
+    wide_inputs(rec[R_CLEARS] + clear_bump(cl), board_ints(nb), (info >> 20) & 1u, in.v);
+    return true;
 }
 
 // One level: every candidate of the segment table, on the fast path or queued
@@ -402,8 +503,8 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality.
 template <bool WIDE>
-__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, bool leaf, uint32_t total,
-                                               int kl, int lane, uint32_t& evals) {
+__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float4* hb, bool leaf,
+                                               uint32_t total, int kl, int lane, uint32_t& evals) {
     LevelAcc acc{0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
@@ -419,9 +520,26 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
     };
     auto drain = [&](uint32_t n, uint32_t queued) {
         uint64_t key = 0;
-        if (uint32_t(lane) < n) {
+        if constexpr (WIDE) {
+            // the inputs per lane, then the network on all lanes together
+            WideIn in{};
+            uint32_t entry = 0;
+            bool legal = false;
+            if (uint32_t(lane) < n) {
+                entry = ws.defer[lane];
+                legal = full_inputs_wide(&ws, lut, entry, in);
+                if (!legal) in = WideIn{};
+            }
+            __syncwarp();
+            float const v = wide_value(in, ws.wglobal, hb, lane);
+            if (legal) {
+                uint32_t const info = ws.seg_info[entry >> 8];
+                key = candidate_key(leaf, v, info, entry & 0xFFu);
+                consume(key, entry >> 8, info);
+            }
+        } else if (uint32_t(lane) < n) {
             uint32_t const entry = ws.defer[lane];
-            key = full_key<WIDE>(&ws, lut, leaf, entry);
+            key = full_key(&ws, lut, leaf, entry);
             consume(key, entry >> 8, ws.seg_info[entry >> 8]);
         }
         fold(key);
@@ -458,7 +576,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
         for (int u = 0; u < TA3B_ILP; ++u) {
             if (WIDE)
                 st[u] = fast_candidate_wide(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
-                                            (info[u] >> 20) & 1u, ws.wglobal, v[u]);
+                                            (info[u] >> 20) & 1u, ws.wglobal, hb, lane, v[u]);
             else
                 st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
                                        (info[u] >> 20) & 1u, fw, v[u]);
@@ -556,7 +674,7 @@ __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
 template <bool WIDE>
-__device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, int lane, uint32_t& evals,
+__device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float4* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
     Move mv{0, 0, 0, true};
     if (ws.eng.over) return mv;
@@ -597,8 +715,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
         // ---- every candidate of the stage
-        LevelAcc const a = level_pass<WIDE>(ws, lut, fw, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane,
-                                            evals);
+        LevelAcc const a = level_pass<WIDE>(ws, lut, fw, hb, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2),
+                                             lane, evals);
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
             kept = __popc(__ballot_sync(FULL_MASK, a.list != 0));
@@ -681,6 +799,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     Luts const lut{s_lut.fast, s_lut.move};
     int const lane = int(threadIdx.x & 31u);
     WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
+    // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
+    float4* const hb = WIDE ? reinterpret_cast<float4*>(dyn_smem + WARPS * sizeof(WarpShared)) +
+                                  (threadIdx.x >> 5) * WIDE_HB_FLOAT4
+                            : nullptr;
     // time budget, measured from this warp's start (the persistent grid starts every warp at launch);
     // kept in shared memory so it costs no register in the move loop
     if (BUDGET && lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ws.t_start));
@@ -711,7 +833,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         __syncwarp();
         uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move<WIDE>(ws, lut, fw, lane, evals, &p.scratch[1]);
+            Move const mv = search_move<WIDE>(ws, lut, fw, hb, lane, evals, &p.scratch[1]);
             if (mv.none) break;
             if (lane == 0) {
                 if (p.trace) {
@@ -790,13 +912,24 @@ __global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand,
     full_v[t] = full_legal[t] ? value_full(rec[R_CLEARS] + clear_bump(cl), board_ints(nb), held, GlobalW{w}) : 0.0f;
 }
 
-// widened models -> their padded device layout (WIDE_STRIDE floats per model)
+// widened models -> their device layout (WIDE_STRIDE floats per model: layers 1
+// and 2 transposed, WIDE_SKIP = 1 when zero terms may be left out). One block per model.
 __global__ void repack_wide_kernel(float const* __restrict__ src, uint32_t models, float* __restrict__ dst) {
-    size_t const i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i >= size_t(models) * WIDE_STRIDE) return;
-    size_t const m = i / WIDE_STRIDE, j = i % WIDE_STRIDE;
-    dst[i] = j < size_t(NPARAMS_WIDE) ? src[m * NPARAMS_WIDE + j] : 0.0f;
+    uint32_t const m = blockIdx.x;
+    if (m >= models) return;
+    float const* s = src + size_t(m) * NPARAMS_WIDE;
+    float* d = dst + size_t(m) * WIDE_STRIDE;
+    int ok = 1;
+    for (int j = int(threadIdx.x); j < NPARAMS_WIDE; j += int(blockDim.x)) {
+        float const x = s[j];
+        ok &= isfinite(x) && !(wide_is_bias(j) && x == 0.0f && signbit(x));
+        d[wide_device_index(j)] = x;
+    }
+    ok = __syncthreads_and(ok);
+    if (threadIdx.x < uint32_t(WIDE_STRIDE - WIDE_SKIP))
+        reinterpret_cast<uint32_t*>(d)[WIDE_SKIP + threadIdx.x] = threadIdx.x == 0 && ok ? 1u : 0u;
 }
+constexpr uint32_t kRepackThreads = 256;
 
 // Launch-shape variants (warps per block, minimum resident blocks per SM =
 // the register cap): the autotuner's search space.
@@ -814,6 +947,8 @@ Variant const kVariants[] = {
     {eval_kernel<10, 2>, 10, 2}, {eval_kernel<20, 1>, 20, 1},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
+// dynamic shared memory per warp: its WarpShared block, plus the widened network's hidden-unit buffer
+constexpr size_t warp_bytes(bool wide) { return sizeof(WarpShared) + (wide ? WIDE_HB_FLOAT4 * sizeof(float4) : 0); }
 // the widened network: ~10,000 FP32 operations per candidate, more registers per lane
 Variant const kWideVariants[] = {
     {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
@@ -910,7 +1045,7 @@ int check_sizes(ta3b_ctx* ctx, uint32_t num_islands, uint32_t models_per_island,
 int setup_wide(ta3b_ctx* ctx) {
     if (ctx->wide_variant >= 0) return TA3B_OK;
     Variant const& v = kWideVariants[kDefaultWideVariant];
-    size_t const dyn = v.warps * sizeof(WarpShared);
+    size_t const dyn = v.warps * warp_bytes(true);
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                         cudaSharedmemCarveoutMaxShared), "smem carveout");
@@ -926,7 +1061,7 @@ int setup_wide(ta3b_ctx* ctx) {
 int setup_budget(ta3b_ctx* ctx, bool wide) {
     if (ctx->budget_grid[wide]) return TA3B_OK;
     Variant const& v = wide ? kBudgetWide : kBudgetV11;
-    size_t const dyn = v.warps * sizeof(WarpShared);
+    size_t const dyn = v.warps * warp_bytes(wide);
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                         cudaSharedmemCarveoutMaxShared), "smem carveout");
@@ -954,7 +1089,7 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, bool wide = false)
     KernelFn const fn = bv ? bv->fn : wide ? kWideVariants[ctx->wide_variant].fn : kVariants[ctx->variant].fn;
     Params p2 = prm;
     p2.budget_ns = ctx->budget_ns;
-    fn<<<grid, warps * 32, warps * sizeof(WarpShared), st>>>(p2);
+    fn<<<grid, warps * 32, warps * warp_bytes(wide), st>>>(p2);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     return TA3B_OK;
 }
@@ -980,8 +1115,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     if (sims == 0) return TA3B_OK;
     if (!weights || !seeds || !score_out) return fail(ctx, TA3B_ERR_ARG, "null weights / seeds / score_out");
     TA3B_CUDA(ctx, cudaSetDevice(ctx->device), "set device");
-    if (num_params == NPARAMS)
-        if (int rc = grow(ctx, ctx->d_w, ctx->cap_w, models * num_params, "alloc weights")) return rc;
+    if (int rc = grow(ctx, ctx->d_w, ctx->cap_w, models * num_params, "alloc weights")) return rc;
     if (int rc = grow(ctx, ctx->d_seeds, ctx->cap_seeds, uint64_t(num_islands) * num_games, "alloc seeds")) return rc;
     if (ctx->cap_sims < sims) {
         size_t c = ctx->cap_sims;
@@ -1008,11 +1142,12 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
         }
     }
     bool const wide = num_params == NPARAMS_WIDE;
-    if (wide) {
+    if (wide) {   // the models as given (d_w), then their device layout (d_wpad)
         if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * WIDE_STRIDE, "alloc padded weights")) return rc;
-        TA3B_CUDA(ctx, cudaMemcpy2DAsync(ctx->d_wpad, WIDE_STRIDE * sizeof(float), weights, NPARAMS_WIDE * sizeof(float),
-                                         NPARAMS_WIDE * sizeof(float), models, cudaMemcpyHostToDevice, ctx->stream),
-                  "copy weights");
+        TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float), cudaMemcpyHostToDevice,
+                                       ctx->stream), "copy weights");
+        repack_wide_kernel<<<uint32_t(models), kRepackThreads, 0, ctx->stream>>>(ctx->d_w, uint32_t(models), ctx->d_wpad);
+        TA3B_CUDA(ctx, cudaGetLastError(), "repack widened weights");
     } else {
         TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float),
                                        cudaMemcpyHostToDevice, ctx->stream), "copy weights");
@@ -1193,8 +1328,7 @@ int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands
     if (wide) {   // the padded copy (allocated on the first widened call of this size)
         uint64_t const models = uint64_t(num_islands) * models_per_island;
         if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * WIDE_STRIDE, "alloc padded weights")) return rc;
-        uint64_t const n = models * WIDE_STRIDE;
-        repack_wide_kernel<<<uint32_t((n + 255) / 256), 256, 0, st>>>(d_weights, uint32_t(models), ctx->d_wpad);
+        repack_wide_kernel<<<uint32_t(models), kRepackThreads, 0, st>>>(d_weights, uint32_t(models), ctx->d_wpad);
         TA3B_CUDA(ctx, cudaGetLastError(), "repack widened weights");
     }
     Params prm{};
