@@ -1042,15 +1042,39 @@ int check_sizes(ta3b_ctx* ctx, uint32_t num_islands, uint32_t models_per_island,
     return TA3B_OK;
 }
 
+// The widened kernels read each model's 19.7 KB of weights through L1, which
+// shares its on-chip memory with shared memory: ask for just the shared memory
+// that min_blocks resident blocks need, so the rest stays L1 (a 20k-sim
+// generation on B200: 24.7 s with the maximum shared-memory split, 20.6 s with
+// this one). Handing each SM its own contiguous range of sims, so that its warps
+// share models, measured slower (26.1 s) than the single queue.
+int set_min_carveout(ta3b_ctx* ctx, Variant const& v, size_t dyn) {
+    int per_sm = 0, reserved = 0;
+    TA3B_CUDA(ctx, cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, ctx->device), "smem per SM");
+    TA3B_CUDA(ctx, cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, ctx->device),
+              "reserved smem per block");
+    cudaFuncAttributes fa{};
+    TA3B_CUDA(ctx, cudaFuncGetAttributes(&fa, v.fn), "kernel attributes");
+    size_t const need = size_t(v.min_blocks) * (dyn + fa.sharedSizeBytes + size_t(reserved));
+    int const pct = per_sm > 0 ? int((need * 100 + size_t(per_sm) - 1) / size_t(per_sm)) : 100;
+    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout, pct < 100 ? pct : 100),
+              "smem carveout");
+    return TA3B_OK;
+}
+
 int setup_wide(ta3b_ctx* ctx) {
     if (ctx->wide_variant >= 0) return TA3B_OK;
     Variant const& v = kWideVariants[kDefaultWideVariant];
     size_t const dyn = v.warps * warp_bytes(true);
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
-    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        cudaSharedmemCarveoutMaxShared), "smem carveout");
+    if (int rc = set_min_carveout(ctx, v, dyn)) return rc;
     int per_sm = 0;
     TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
+    if (per_sm < int(v.min_blocks)) {   // the split chosen leaves too little shared memory: take the maximum
+        TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            cudaSharedmemCarveoutMaxShared), "smem carveout");
+        TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
+    }
     if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "widened kernel does not fit on an SM");
     ctx->wide_variant = kDefaultWideVariant;
     ctx->wide_warps = v.warps;
@@ -1063,10 +1087,19 @@ int setup_budget(ta3b_ctx* ctx, bool wide) {
     Variant const& v = wide ? kBudgetWide : kBudgetV11;
     size_t const dyn = v.warps * warp_bytes(wide);
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
-    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                        cudaSharedmemCarveoutMaxShared), "smem carveout");
+    if (wide) {
+        if (int rc = set_min_carveout(ctx, v, dyn)) return rc;
+    } else {
+        TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            cudaSharedmemCarveoutMaxShared), "smem carveout");
+    }
     int per_sm = 0;
     TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
+    if (wide && per_sm < int(v.min_blocks)) {
+        TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                            cudaSharedmemCarveoutMaxShared), "smem carveout");
+        TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
+    }
     if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "budget kernel does not fit on an SM");
     ctx->budget_grid[wide] = ctx->sms * uint32_t(per_sm);
     return TA3B_OK;
