@@ -165,8 +165,9 @@ int ta3b_select_variant(ta3b_ctx* ctx, int variant);
 int ta3b_core_selftest(const uint32_t* recs, uint32_t num_recs, const uint32_t* cand, uint32_t n, const float* w97,
                        float* fast_v, int* fast_st, float* full_v, int* full_legal, float* dbg32);
 
-/* Launch shape the context uses (after the first evaluation): grid blocks,
- * warps per block, sims per launch. For tooling and the autotuner. */
+/* Launch shape of the context's most recent kernel launch (before the first
+ * one: the selected variant's full grid): grid blocks, warps per block, and the
+ * device's SM count. For tooling and the autotuner. */
 int ta3b_launch_info(const ta3b_ctx* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms);
 
 #ifdef __cplusplus

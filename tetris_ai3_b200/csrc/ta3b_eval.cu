@@ -249,13 +249,13 @@ __device__ __forceinline__ int fast_candidate(uint32_t const* __restrict__ rec, 
 // are all finite and whose biases are not -0; every other model runs every term.
 // Each unit's sum keeps the reference order (utility.hpp:30-46: bias, then the
 // inputs ascending), only without the zero terms. Lanes without a candidate pass
-// zero inputs. hb: this warp's hidden-unit buffer, [unit / 4][lane] float4.
+// zero inputs. hb: this warp's hidden-unit buffer, [unit][lane] floats (no bank conflicts).
 struct WideIn {
     float v[NIN];
 };
-constexpr int WIDE_HB_FLOAT4 = WH / 4 * WARP;          // per warp: 64 units x 32 lanes (8 KB)
+constexpr int WIDE_HB_FLOATS = WH * WARP;              // per warp: 64 units x 32 lanes (8 KB)
 
-__device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w, float4* __restrict__ hb, int lane) {
+__device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w, float* __restrict__ hb, int lane) {
     uint32_t const skip = __ldg(reinterpret_cast<uint32_t const*>(w) + WIDE_SKIP);
     float a[WH];
 #pragma unroll
@@ -287,7 +287,11 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
 #pragma unroll
     for (int o = 0; o < WH; o += 4) {
         float4 const h = make_float4(relu(a[o]), relu(a[o + 1]), relu(a[o + 2]), relu(a[o + 3]));
-        hb[(o / 4) * WARP + lane] = h;
+        float* const hq = hb + lane;
+        hq[(o + 0) * WARP] = h.x;
+        hq[(o + 1) * WARP] = h.y;
+        hq[(o + 2) * WARP] = h.z;
+        hq[(o + 3) * WARP] = h.w;
         uint32_t const bits = (h.x != 0.0f ? 1u : 0u) | (h.y != 0.0f ? 2u : 0u) | (h.z != 0.0f ? 4u : 0u) |
                               (h.w != 0.0f ? 8u : 0u);
         nz[o >> 5] |= bits << (o & 31);
@@ -304,12 +308,12 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
         float4 const b = __ldg(reinterpret_cast<float4 const*>(w + WIDE_B2 + o));
         a[o] = b.x; a[o + 1] = b.y; a[o + 2] = b.z; a[o + 3] = b.w;
     }
-    float const* hs = reinterpret_cast<float const*>(hb) + 4 * lane;
+    float const* hs = hb + lane;
     uint64_t m = (uint64_t(nz[1]) << 32) | nz[0];
     while (m) {
         int const i = __ffsll(static_cast<long long>(m)) - 1;
         m &= m - 1;
-        float const x = hs[(i >> 2) * (4 * WARP) + (i & 3)];
+        float const x = hs[i * WARP];
         float4 const* wr = reinterpret_cast<float4 const*>(w + WIDE_W2T + i * WH);
 #pragma unroll
         for (int o = 0; o < WH; o += 4) {
@@ -335,7 +339,7 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
 
 // fast path of the widened network: the same record words; every lane of the warp calls it
 __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ rec, PlaceFast pf, bool held_i,
-                                                   float const* __restrict__ w, float4* hb, int lane, float& v) {
+                                                   float const* __restrict__ w, float* hb, int lane, float& v) {
     RecView r;
     uint4 const q = *reinterpret_cast<uint4 const*>(rec + R_HD);
     r.hd = q.x; r.rc0 = q.y; r.rc1 = q.z; r.rc2 = q.w;
@@ -503,7 +507,7 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality.
 template <bool WIDE>
-__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float4* hb, bool leaf,
+__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float* hb, bool leaf,
                                                uint32_t total, int kl, int lane, uint32_t& evals) {
     LevelAcc acc{0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
@@ -674,7 +678,7 @@ __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
 template <bool WIDE>
-__device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float4* hb, int lane, uint32_t& evals,
+__device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
     Move mv{0, 0, 0, true};
     if (ws.eng.over) return mv;
@@ -800,9 +804,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     int const lane = int(threadIdx.x & 31u);
     WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
     // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
-    float4* const hb = WIDE ? reinterpret_cast<float4*>(dyn_smem + WARPS * sizeof(WarpShared)) +
-                                  (threadIdx.x >> 5) * WIDE_HB_FLOAT4
-                            : nullptr;
+    float* const hb = WIDE ? reinterpret_cast<float*>(dyn_smem + WARPS * sizeof(WarpShared)) +
+                                 (threadIdx.x >> 5) * WIDE_HB_FLOATS
+                           : nullptr;
     // time budget, measured from this warp's start (the persistent grid starts every warp at launch);
     // kept in shared memory so it costs no register in the move loop
     if (BUDGET && lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ws.t_start));
@@ -948,7 +952,7 @@ Variant const kVariants[] = {
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // dynamic shared memory per warp: its WarpShared block, plus the widened network's hidden-unit buffer
-constexpr size_t warp_bytes(bool wide) { return sizeof(WarpShared) + (wide ? WIDE_HB_FLOAT4 * sizeof(float4) : 0); }
+constexpr size_t warp_bytes(bool wide) { return sizeof(WarpShared) + (wide ? WIDE_HB_FLOATS * sizeof(float) : 0); }
 // the widened network: ~10,000 FP32 operations per candidate, more registers per lane
 Variant const kWideVariants[] = {
     {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
@@ -997,6 +1001,7 @@ struct ta3b_ctx {
     int wide_variant = -1;            // widened-network kernel, set up on first use
     uint32_t budget_grid[2] = {0, 0};  // budget flavours (v11, widened), set up on first use
     uint32_t wide_warps = 0, wide_grid = 0;
+    uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
     std::string err;
 };
 
@@ -1124,6 +1129,8 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, bool wide = false)
     p2.budget_ns = ctx->budget_ns;
     fn<<<grid, warps * 32, warps * warp_bytes(wide), st>>>(p2);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
+    ctx->last_grid = grid;
+    ctx->last_warps = warps;
     return TA3B_OK;
 }
 
@@ -1460,8 +1467,8 @@ int ta3b_select_variant(ta3b_ctx* ctx, int variant) {
 
 int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms) {
     if (!ctx) return TA3B_ERR_ARG;
-    if (grid) *grid = ctx->grid;
-    if (warps_per_block) *warps_per_block = ctx->warps_per_block;
+    if (grid) *grid = ctx->last_grid ? ctx->last_grid : ctx->grid;
+    if (warps_per_block) *warps_per_block = ctx->last_grid ? ctx->last_warps : ctx->warps_per_block;
     if (sms) *sms = ctx->sms;
     return TA3B_OK;
 }
