@@ -345,7 +345,8 @@ def run_ours(args):
                 "clocks": clocks, "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps},
-                "gpu_launches": args.steps}
+                # per step: the evaluation kernel (the widened model adds its weight-repack kernel)
+                "gpu_launches": args.steps * (2 if wide else 1)}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
