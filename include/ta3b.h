@@ -98,9 +98,10 @@ int ta3b_eval_islands(ta3b_ctx* ctx, const float* weights, uint32_t num_islands,
  * synchronised. evals_out (may be NULL) receives per-sim counts of evaluated
  * beam placements (value-model calls). Used for HBM-resident batches and CUDA
  * graph capture. With the widened network (num_params = TA3B_NUM_PARAMS_WIDE)
- * the call first repacks the weights into a 16-byte-aligned copy owned by the
- * context; that copy is allocated by the first widened call of a larger size,
- * so make such a call once before capturing it. No reference counterpart (the
+ * the call first repacks the weights into the kernel's layout (16-byte aligned,
+ * layers 1 and 2 transposed, a per-model flag) in a copy owned by the context;
+ * that copy is allocated by the first widened call of a larger size, so make
+ * such a call once before capturing it. No reference counterpart (the
  * reference stages host buffers). */
 int ta3b_eval_device(ta3b_ctx* ctx, const float* d_weights, uint32_t num_islands, uint32_t models_per_island,
                      uint32_t num_params, const uint64_t* d_seeds, uint32_t num_games, uint32_t max_moves,
