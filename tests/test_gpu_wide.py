@@ -113,3 +113,23 @@ def test_wide_device_entry_matches_host_entry(ev):
     ev.eval_device(dw, ds, cap, score)
     torch.cuda.synchronize()
     assert score.cpu().numpy().tobytes() == host.tobytes()
+
+
+def test_wide_time_budget_flavour(ev):
+    """The widened network's budget-checking kernel: a generous budget scores
+    the batch exactly like the ordinary kernel; a budget far below the run time
+    ends the launch with TA3B_ERR_TIMEOUT and leaves the context usable."""
+    from tetris_ai3_b200 import EvaluatorError
+    w, seeds, cap = _variant_models()
+    ref = ev.eval_full(w, w.shape[0], seeds, cap)
+    try:
+        ev.set_time_budget(120.0)
+        full = ev.eval_full(w, w.shape[0], seeds, cap)
+        assert all(x.tobytes() == y.tobytes() for x, y in zip(ref, full))
+        ev.set_time_budget(1e-5)
+        with pytest.raises(EvaluatorError, match="time budget"):
+            ev.eval_full(w, w.shape[0], seeds, 2000)
+    finally:
+        ev.set_time_budget(0)
+    again = ev.eval_full(w, w.shape[0], seeds, cap)
+    assert all(x.tobytes() == y.tobytes() for x, y in zip(ref, again))
