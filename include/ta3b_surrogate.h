@@ -49,6 +49,39 @@ int ta3s_train(ta3s_model* m, uint32_t epochs, uint32_t batch, float lr, float w
  * before the next ta3s_train. */
 int ta3s_predict(ta3s_model* m, const float* x, uint32_t n, float* mean_out, float* logvar_out);
 
+/* ---- the same scheme for any parameter-vector size (ta3w_*) ----
+ * MLP in -> H -> H -> 2 for the widened evaluator's 4,929-parameter vectors
+ * (H = 256) or any other size: in_dim >= 1, H a multiple of 128. Each matrix
+ * product is one launch of a tcgen05 BF16 GEMM kernel (FP32 accumulation in
+ * tensor memory, split-K for the first layer); bias, ReLU, output layer, loss and
+ * bias gradients in FP32 on the CUDA cores. Rounding points (BF16, nearest
+ * even): standardised inputs, W1, W2, relu(H1), dH2, dH1; everything else FP32.
+ * Parameter vector (ta3w_num_params(in_dim, H) values), INP = in_dim rounded up
+ * to a multiple of 128:
+ *   W1 [H][INP] (columns in_dim.. are zero padding), W2 [H][H], W3 [2][H],
+ *   b1 [H], b2 [H], b3 [2]. Gradients use the same layout.
+ * Calls mirror the ta3s_* functions above. A model is not thread-safe. */
+typedef struct ta3w_model ta3w_model;
+
+uint32_t ta3w_num_params(uint32_t in_dim, uint32_t hidden);   /* 0 for unsupported sizes */
+ta3w_model* ta3w_create(int device, uint32_t in_dim, uint32_t hidden, uint32_t seed);
+void ta3w_destroy(ta3w_model* m);
+const char* ta3w_last_error(const ta3w_model* m);
+uint32_t ta3w_model_params(const ta3w_model* m);
+int ta3w_set_params(ta3w_model* m, const float* params);     /* also resets the Adam moments */
+int ta3w_get_params(ta3w_model* m, float* params_out);
+int ta3w_set_data(ta3w_model* m, const float* x, const float* y, uint32_t n);   /* x [n][in_dim] */
+int ta3w_set_data_standardized(ta3w_model* m, const float* x, const float* y, uint32_t n);
+int ta3w_gradients(ta3w_model* m, float* grad_out, float* loss_sum_out);
+int ta3w_train(ta3w_model* m, uint32_t epochs, uint32_t batch, float lr, float weight_decay, uint32_t seed,
+               float* final_loss);
+int ta3w_predict(ta3w_model* m, const float* x, uint32_t n, float* mean_out, float* logvar_out);
+/* Test hook: the GEMM kernel alone on host BF16 bit patterns. c [m][n] =
+ * sum_k A(m, k) B(n, k) with A given as [m][k] (a_mn = 0) or [k][m] (a_mn = 1)
+ * and B as [n][k] or [k][n]; m, n multiples of 128, k of 64; K split `splits` ways. */
+int ta3w_gemm_test(int device, int a_mn, int b_mn, int m, int n, int k, int splits, const uint16_t* a,
+                   const uint16_t* b, float* c);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,7 +25,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # also spells the roundings out with __fmul_rn / __fadd_rn.
 NVCC_FLAGS = ["-O3", "-std=c++20", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-shared",
               "--expt-relaxed-constexpr", "-Xptxas", "-v"]
-SOURCES = ["ta3b_eval.cu", "ta3s_surrogate.cu"]
+SOURCES = ["ta3b_eval.cu", "ta3s_surrogate.cu", "ta3s_wide.cu"]
 
 
 def nvcc() -> str:

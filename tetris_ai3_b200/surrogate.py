@@ -1,7 +1,9 @@
 """Python binding of the GPU surrogate model (include/ta3b_surrogate.h, in
-libta3b.so): an MLP 97 -> 128 -> 128 -> 2 trained on (parameter vector ->
-mean score) pairs with hand-written tcgen05 forward / backward / Adam kernels.
-`train(x, y)` / `predict(x)` make it usable as the island trainer's surrogate."""
+libta3b.so): an MLP in_dim -> hidden -> hidden -> 2 (97 -> 128 -> 128 -> 2 for
+v11, 4929 -> 256 -> 256 -> 2 for the widened evaluator) trained on (parameter
+vector -> mean score) pairs with hand-written tcgen05 forward / backward / Adam
+kernels. `train(x, y)` / `predict(x)` make it usable as the island trainer's
+surrogate."""
 from __future__ import annotations
 
 import ctypes as C
@@ -22,8 +24,24 @@ _SIG = {
     "ta3s_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
     "ta3s_train": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.c_void_p]),
     "ta3s_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    # any parameter-vector size (the widened evaluator's 4,929)
+    "ta3w_num_params": (C.c_uint32, [C.c_uint32, C.c_uint32]),
+    "ta3w_create": (C.c_void_p, [C.c_int, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "ta3w_destroy": (None, [C.c_void_p]),
+    "ta3w_last_error": (C.c_char_p, [C.c_void_p]),
+    "ta3w_model_params": (C.c_uint32, [C.c_void_p]),
+    "ta3w_set_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ta3w_get_params": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "ta3w_set_data": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "ta3w_set_data_standardized": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]),
+    "ta3w_gradients": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ta3w_train": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.c_void_p]),
+    "ta3w_predict": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "ta3w_gemm_test": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                 C.c_void_p, C.c_void_p]),
 }
 SURROGATE_EXPORTS = sorted(_SIG)
+V11_SHAPE = (97, 128)            # the fused single-kernel model (ta3s_*)
 
 
 def _lib():
@@ -39,59 +57,72 @@ def _p(a):
 
 
 class Surrogate:
-    """The GPU surrogate. Raises EvaluatorError without an sm_100 device."""
+    """The GPU surrogate: in_dim -> hidden -> hidden -> 2. The v11 shape (97, 128)
+    runs the fused kernel (ta3s_*); any other shape, e.g. the widened evaluator's
+    (4929, 256), the layer-by-layer GEMM path (ta3w_*). Raises EvaluatorError
+    without an sm_100 device."""
 
     def __init__(self, device: int = 0, seed: int = 0, epochs: int = 40, batch: int = 256, lr: float = 1e-3,
-                 weight_decay: float = 1e-2):
+                 weight_decay: float = 1e-2, in_dim: int = 97, hidden: int = 128):
         self.lib = _lib()
-        self.h = self.lib.ta3s_create(device, seed)
+        self.in_dim, self.hidden = in_dim, hidden
+        self.fused = (in_dim, hidden) == V11_SHAPE
+        self._pre = "ta3s_" if self.fused else "ta3w_"
+        if self.fused:
+            self.h = self.lib.ta3s_create(device, seed)
+        else:
+            self.h = self.lib.ta3w_create(device, in_dim, hidden, seed)
         if not self.h:
-            raise EvaluatorError(self.lib.ta3s_last_error(None).decode())
-        self.nparam = int(self.lib.ta3s_num_params())
+            raise EvaluatorError(self._f("last_error")(None).decode())
+        self.nparam = int(self.lib.ta3s_num_params() if self.fused else self.lib.ta3w_model_params(self.h))
         self.epochs, self.batch, self.lr, self.wd, self.seed = epochs, batch, lr, weight_decay, seed
         self.trainings = 0
         self.last_loss = float("nan")
 
+    def _f(self, name):
+        return getattr(self.lib, self._pre + name)
+
     def __del__(self):
         if getattr(self, "h", None):
-            self.lib.ta3s_destroy(self.h)
+            self._f("destroy")(self.h)
             self.h = None
 
     def _ok(self, rc):
         if rc:
-            raise EvaluatorError(self.lib.ta3s_last_error(self.h).decode())
+            raise EvaluatorError(self._f("last_error")(self.h).decode())
 
     @property
     def params(self) -> np.ndarray:
         out = np.empty(self.nparam, np.float32)
-        self._ok(self.lib.ta3s_get_params(self.h, _p(out)))
+        self._ok(self._f("get_params")(self.h, _p(out)))
         return out
 
     @params.setter
     def params(self, p):
         p = np.ascontiguousarray(p, np.float32)
         assert p.size == self.nparam
-        self._ok(self.lib.ta3s_set_params(self.h, _p(p)))
+        self._ok(self._f("set_params")(self.h, _p(p)))
+
+    def _set_data(self, x, y, standardized: bool):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        assert x.ndim == 2 and x.shape[1] == self.in_dim and len(y) == len(x)
+        fn = self._f("set_data_standardized" if standardized else "set_data")
+        self._ok(fn(self.h, _p(x), _p(y), len(y)))
 
     def gradients(self, x, y, standardized: bool = True):
         """Gradient of the mean loss over (x, y) and the summed loss, no update."""
-        x = np.ascontiguousarray(x, np.float32)
-        y = np.ascontiguousarray(y, np.float32)
-        fn = self.lib.ta3s_set_data_standardized if standardized else self.lib.ta3s_set_data
-        self._ok(fn(self.h, _p(x), _p(y), len(y)))
+        self._set_data(x, y, standardized)
         g = np.empty(self.nparam, np.float32)
         loss = C.c_float()
-        self._ok(self.lib.ta3s_gradients(self.h, _p(g), C.byref(loss)))
+        self._ok(self._f("gradients")(self.h, _p(g), C.byref(loss)))
         return g, loss.value
 
     def train(self, x, y, epochs: int | None = None, batch: int | None = None, standardized: bool = False):
-        x = np.ascontiguousarray(x, np.float32)
-        y = np.ascontiguousarray(y, np.float32)
-        fn = self.lib.ta3s_set_data_standardized if standardized else self.lib.ta3s_set_data
-        self._ok(fn(self.h, _p(x), _p(y), len(y)))
+        self._set_data(x, y, standardized)
         loss = C.c_float()
-        self._ok(self.lib.ta3s_train(self.h, epochs or self.epochs, batch or self.batch, self.lr, self.wd,
-                                     self.seed + self.trainings, C.byref(loss)))
+        self._ok(self._f("train")(self.h, epochs or self.epochs, batch or self.batch, self.lr, self.wd,
+                                  self.seed + self.trainings, C.byref(loss)))
         self.trainings += 1
         self.last_loss = loss.value
         return loss.value
@@ -101,8 +132,20 @@ class Surrogate:
         n = len(x)
         mean = np.empty(n, np.float32)
         lv = np.empty(n, np.float32) if with_logvar else None
-        self._ok(self.lib.ta3s_predict(self.h, _p(x), n, _p(mean), _p(lv)))
+        self._ok(self._f("predict")(self.h, _p(x), n, _p(mean), _p(lv)))
         return (mean, lv) if with_logvar else mean
+
+
+def gemm_test(a, b, a_mn: bool, b_mn: bool, m: int, n: int, k: int, splits: int = 1, device: int = 0):
+    """The surrogate's tcgen05 GEMM kernel alone: a, b are BF16 bit patterns (uint16)
+    in their global layouts; returns C [m][n] = sum_k A(m, k) B(n, k) (FP32)."""
+    lib = _lib()
+    a = np.ascontiguousarray(a, np.uint16)
+    b = np.ascontiguousarray(b, np.uint16)
+    c = np.empty((m, n), np.float32)
+    if lib.ta3w_gemm_test(device, int(a_mn), int(b_mn), m, n, k, splits, _p(a), _p(b), _p(c)):
+        raise EvaluatorError(lib.ta3w_last_error(None).decode())
+    return c
 
 
 def main(argv=None):
