@@ -21,7 +21,9 @@
  * the latest generation, which is held out; while its
  * Spearman rho on that held-out slice is below `surrogate_min_rho` the
  * generation runs without pre-screening. Every fitness the trainer reports
- * comes from full evaluation. */
+ * comes from full evaluation. Without a caller-supplied surrogate the built-in
+ * GPU model is used: 97 -> 128 -> 128 -> 2 (ta3s_*) for v11's 97 parameters,
+ * num_params -> 256 -> 256 -> 2 (ta3w_*) for any other size. */
 #ifndef TA3B_TRAINER_H
 #define TA3B_TRAINER_H
 

@@ -58,3 +58,31 @@ def test_widened_trainer_on_gpu_equals_trainer_on_oracle(host, oracle):
         xc, fc = cpu.champion(i)
         assert fg == fc and np.array_equal(xg, xc)
     assert gpu.stats()["pieces"] == cpu.stats()["pieces"]
+
+
+@pytest.mark.parametrize("num_params", [97, 4929])
+def test_built_in_gpu_surrogate_prescreens(host, num_params):
+    """The trainer's own GPU surrogate (97 -> 128 -> 128 -> 2 for v11, 4929 -> 256 ->
+    256 -> 2 for the widened vector) on a quadratic landscape: it retrains on the
+    archive and gates itself on held-out rank correlation; the 97-parameter model
+    passes the gate and pre-screens the later generations."""
+    target = np.linspace(-0.5, 0.5, num_params)
+
+    def score(w, seeds, mm):
+        base = -((w.astype(np.float64) - target) ** 2).sum(1)
+        return (base[:, None] + np.zeros(len(seeds))[None, :]).astype(np.float32)
+
+    cfg = host.default_config(islands=2, population=16, gens_per_iteration=3, iterations_per_cycle=2, games=2,
+                              max_moves=50, algo=host.SEP, num_params=num_params, sigma0=0.3,
+                              surrogate_start_gen=6, surrogate_sample=32, surrogate_top=8, surrogate_random=2,
+                              surrogate_retrain=2, surrogate_min_rho=0.3, surrogate_epochs=30, surrogate_batch=64)
+    t = host.Trainer(cfg, score=score)
+    for _ in range(10):
+        t.run_generation()
+    st = t.stats()
+    assert st["surrogate_trainings"] >= 2 and np.isfinite(st["last_rho"])
+    sizes = [n for n, _, _ in t.calls]
+    assert sizes[:6] == [2 * 16] * 6                 # start-up and generations 1..5: full evaluation
+    assert set(sizes[6:]) <= {2 * 16, 2 * 10}        # then full, or pre-screened (8 + 2 per island)
+    if num_params == 97:                             # the small model learns this landscape and screens
+        assert st["surrogate_active"] == 1 and 2 * 10 in sizes[6:]

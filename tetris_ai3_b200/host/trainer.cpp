@@ -113,25 +113,34 @@ double spearman(std::vector<double> const& a, std::vector<double> const& b) {
     return sab / std::sqrt(saa * sbb);
 }
 
-// the built-in surrogate: the GPU MLP behind include/ta3b_surrogate.h
+// the built-in surrogate: the GPU MLP behind include/ta3b_surrogate.h, 97 -> 128 ->
+// 128 -> 2 for v11's parameter vectors, num_params -> 256 -> 256 -> 2 for any other size
+constexpr uint32_t kV11Params = 97, kWideSurrogateHidden = 256;
 struct GpuSurrogate {
     ta3s_model* model = nullptr;
+    ta3w_model* wide = nullptr;
     uint32_t epochs = 40, batch = 256, trainings = 0;
     float lr = 1e-3f, weight_decay = 1e-2f;
     ~GpuSurrogate() {
         if (model) ta3s_destroy(model);
+        if (wide) ta3w_destroy(wide);
     }
 };
 
 int gpu_sur_train(void* user, const float* x, const float* y, uint32_t n, uint32_t) {
     auto* s = static_cast<GpuSurrogate*>(user);
-    if (ta3s_set_data(s->model, x, y, n)) return 1;
     float loss = 0.f;
-    return ta3s_train(s->model, s->epochs, s->batch, s->lr, s->weight_decay, 0x5A11u + s->trainings++, &loss);
+    uint32_t const seed = 0x5A11u + s->trainings++;
+    if (s->wide)
+        return ta3w_set_data(s->wide, x, y, n) ||
+               ta3w_train(s->wide, s->epochs, s->batch, s->lr, s->weight_decay, seed, &loss);
+    if (ta3s_set_data(s->model, x, y, n)) return 1;
+    return ta3s_train(s->model, s->epochs, s->batch, s->lr, s->weight_decay, seed, &loss);
 }
 
 int gpu_sur_predict(void* user, const float* x, uint32_t n, uint32_t, float* mean_out) {
-    return ta3s_predict(static_cast<GpuSurrogate*>(user)->model, x, n, mean_out, nullptr);
+    auto* s = static_cast<GpuSurrogate*>(user);
+    return s->wide ? ta3w_predict(s->wide, x, n, mean_out, nullptr) : ta3s_predict(s->model, x, n, mean_out, nullptr);
 }
 
 // the built-in score function: the GPU evaluator behind include/ta3b.h
@@ -232,8 +241,13 @@ struct ta3t_trainer {
         if (cfg.algo != TA3C_SEP && cfg.algo != TA3C_DD) return fail("ta3t_create: algo must be TA3C_SEP or TA3C_DD");
         if (cfg.surrogate_start_gen && !s) {
             gpu_sur = std::make_unique<GpuSurrogate>();
-            gpu_sur->model = ta3s_create(c->device, uint32_t(cfg.training_seed));
-            if (!gpu_sur->model) return fail(std::string("surrogate: ") + ta3s_last_error(nullptr));
+            if (cfg.num_params == kV11Params) {
+                gpu_sur->model = ta3s_create(c->device, uint32_t(cfg.training_seed));
+                if (!gpu_sur->model) return fail(std::string("surrogate: ") + ta3s_last_error(nullptr));
+            } else {
+                gpu_sur->wide = ta3w_create(c->device, cfg.num_params, kWideSurrogateHidden, uint32_t(cfg.training_seed));
+                if (!gpu_sur->wide) return fail(std::string("surrogate: ") + ta3w_last_error(nullptr));
+            }
             if (cfg.surrogate_epochs) gpu_sur->epochs = cfg.surrogate_epochs;
             if (cfg.surrogate_batch) gpu_sur->batch = cfg.surrogate_batch;
             if (cfg.surrogate_lr > 0) gpu_sur->lr = float(cfg.surrogate_lr);
