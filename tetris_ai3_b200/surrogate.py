@@ -150,7 +150,8 @@ def gemm_test(a, b, a_mn: bool, b_mn: bool, m: int, n: int, k: int, splits: int 
 
 def main(argv=None):
     """Time the GPU surrogate on a seeded synthetic (parameters -> score) set:
-    python -m tetris_ai3_b200.surrogate [--rows 8000] [--epochs 40] [--batch 256]"""
+    python -m tetris_ai3_b200.surrogate [--rows 8000] [--epochs 40] [--batch 256]
+                                        [--in-dim 97 --hidden 128 | --in-dim 4929 --hidden 256]"""
     import argparse
     import json
     import time
@@ -159,19 +160,23 @@ def main(argv=None):
     ap.add_argument("--epochs", type=int, default=40)
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--predict", type=int, default=800)
+    ap.add_argument("--in-dim", type=int, default=V11_SHAPE[0])
+    ap.add_argument("--hidden", type=int, default=V11_SHAPE[1])
     args = ap.parse_args(argv)
     rng = np.random.default_rng(0)
-    a = rng.normal(size=(8, 97)) / np.sqrt(97)
-    x = rng.normal(size=(args.rows, 97)).astype(np.float32)
+    a = rng.normal(size=(8, args.in_dim)) / np.sqrt(args.in_dim)
+    x = rng.normal(size=(args.rows, args.in_dim)).astype(np.float32)
     y = (-((x @ a.T) ** 2).sum(1)).astype(np.float32)
-    s = Surrogate(batch=args.batch, epochs=args.epochs)
+    s = Surrogate(batch=args.batch, epochs=args.epochs, in_dim=args.in_dim, hidden=args.hidden)
+    s.train(x[:256], y[:256], epochs=1)                 # warm-up: first launches, buffers
     t0 = time.perf_counter()
     loss = s.train(x, y)
     t1 = time.perf_counter()
     s.predict(x[:args.predict])
     t2 = time.perf_counter()
     steps = args.epochs * ((args.rows + args.batch - 1) // args.batch)
-    print(json.dumps({"rows": args.rows, "epochs": args.epochs, "batch": args.batch, "train_s": t1 - t0,
+    print(json.dumps({"in_dim": args.in_dim, "hidden": args.hidden, "params": s.nparam, "rows": args.rows,
+                      "epochs": args.epochs, "batch": args.batch, "train_s": t1 - t0,
                       "ms_per_step": 1e3 * (t1 - t0) / steps, "predict_ms": 1e3 * (t2 - t1), "final_loss": loss}))
 
 
