@@ -28,10 +28,12 @@ extern "C" {
 
 #define TA3B_NUM_PARAMS 97 /* v11 value model, ta3_ai/incl/ta3/ai/models/models/model_v11.hpp:44 */
 /* The reference's dense layers (ta3_ai/incl/ta3/ai/models/models/utility.hpp:29-46)
- * widened to 10 -> 64 ReLU -> 64 ReLU -> 1 over the same v11 inputs; per layer
- * [out][in] weights then [out] biases. Every evaluation entry point except
- * ta3b_eval_device_noalloc and ta3b_core_selftest accepts it as num_params. */
+ * widened to 10 -> H ReLU -> H ReLU -> 1 over the same v11 inputs; per layer
+ * [out][in] weights then [out] biases. The kernels are built for H = 64 (4,929
+ * parameters) and H = 32 (1,441). Every evaluation entry point except
+ * ta3b_eval_device_noalloc and ta3b_core_selftest accepts them as num_params. */
 #define TA3B_NUM_PARAMS_WIDE 4929
+#define TA3B_NUM_PARAMS_WIDE32 1441
 
 enum {
     TA3B_OK = 0,
@@ -72,7 +74,8 @@ int ta3b_set_time_budget(ta3b_ctx* ctx, double seconds);
 
 /* Batched evaluation with host buffers: num_models models, each played on the
  * SAME num_games seeds. weights is model-major, num_models * num_params floats
- * (num_params: TA3B_NUM_PARAMS, or TA3B_NUM_PARAMS_WIDE for the widened network).
+ * (num_params: TA3B_NUM_PARAMS, or TA3B_NUM_PARAMS_WIDE / TA3B_NUM_PARAMS_WIDE32 for
+ * the widened networks).
  * Outputs are model-major: index
  * m * num_games + g holds model m on game g. pieces_out, lines_out may be NULL.
  * score is the reference's score_v1 (FP64, rounded to float); -1e6 when no

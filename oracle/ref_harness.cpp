@@ -51,22 +51,28 @@ struct game_out {
 
 // The reference's customizable architecture widened: the v11 inputs
 // (ModelV11::extractInputs, model_v11.hpp:63-91) through the reference's own
-// dense layers (utility.hpp:29-46) 10 -> 64 ReLU -> 64 ReLU -> 1, weights of
-// each layer as [out][in] then [out] biases: 704 + 4160 + 65 = 4,929 parameters.
+// dense layers (utility.hpp:29-46) 10 -> H ReLU -> H ReLU -> 1, weights of each
+// layer as [out][in] then [out] biases: H = 64 gives 704 + 4160 + 65 = 4,929
+// parameters, H = 32 gives 1,441.
+template<std::size_t H>
+struct wide_net {
+    static constexpr std::size_t L1 = 10 * H + H, L2 = H * H + H, L3 = H + 1, P = L1 + L2 + L3;
+};
 constexpr std::size_t WIDE_H = 64;
-constexpr std::size_t WIDE_L1 = 10 * WIDE_H + WIDE_H, WIDE_L2 = WIDE_H * WIDE_H + WIDE_H, WIDE_L3 = WIDE_H + 1;
-constexpr std::size_t WIDE_P = WIDE_L1 + WIDE_L2 + WIDE_L3;
+constexpr std::size_t WIDE_P = wide_net<WIDE_H>::P;
 
+template<std::size_t H>
 struct counting_wide {
+    using N = wide_net<H>;
     float const* w;
     std::uint64_t* counter;
     [[nodiscard]] search::value_t evaluate(search::clear_t c, sim::Board2 const& b, bool held_i) const {
         ++*counter;
         std::array<ai::data_t, ai::ModelV11::INPUTS> in{};
         ai::ModelV11::extractInputs(c, b, held_i, in);
-        auto const h1 = ai::dense<10, WIDE_H, true>(in, std::span<ai::data_t const, WIDE_L1>{w, WIDE_L1});
-        auto const h2 = ai::dense<WIDE_H, WIDE_H, true>(h1, std::span<ai::data_t const, WIDE_L2>{w + WIDE_L1, WIDE_L2});
-        return ai::dense<WIDE_H, 1, false>(h2, std::span<ai::data_t const, WIDE_L3>{w + WIDE_L1 + WIDE_L2, WIDE_L3})[0];
+        auto const h1 = ai::dense<10, H, true>(in, std::span<ai::data_t const, N::L1>{w, N::L1});
+        auto const h2 = ai::dense<H, H, true>(h1, std::span<ai::data_t const, N::L2>{w + N::L1, N::L2});
+        return ai::dense<H, 1, false>(h2, std::span<ai::data_t const, N::L3>{w + N::L1 + N::L2, N::L3})[0];
     }
 };
 
@@ -83,11 +89,17 @@ game_out play(float const* w, std::uint64_t seed, std::uint32_t max_moves, std::
     return play_with(model, evals, seed, max_moves, trace, n_moves, board_out);
 }
 
+template<std::size_t H>
+game_out play_wide_h(float const* w, std::uint64_t seed, std::uint32_t max_moves, std::uint8_t* trace,
+                     std::uint32_t* n_moves, std::uint32_t* board_out) {
+    std::uint64_t evals = 0;
+    counting_wide<H> const model{w, &evals};
+    return play_with(model, evals, seed, max_moves, trace, n_moves, board_out);
+}
+
 game_out play_wide(float const* w, std::uint64_t seed, std::uint32_t max_moves, std::uint8_t* trace,
                    std::uint32_t* n_moves, std::uint32_t* board_out) {
-    std::uint64_t evals = 0;
-    counting_wide const model{w, &evals};
-    return play_with(model, evals, seed, max_moves, trace, n_moves, board_out);
+    return play_wide_h<WIDE_H>(w, seed, max_moves, trace, n_moves, board_out);
 }
 
 template<class Model>
@@ -228,6 +240,14 @@ int ta3ref_eval_wide_mt(float const* w, std::uint32_t num_models, std::uint64_t 
                         std::uint32_t* lines_out, std::uint64_t* evals_total) {
     return eval_mt(play_wide, WIDE_P, w, num_models, seeds, num_games, max_moves, threads, score_out, pieces_out,
                    lines_out, evals_total);
+}
+
+// the same batch for the 10 -> 32 -> 32 -> 1 model (1,441 parameters per model)
+int ta3ref_eval_wide32_mt(float const* w, std::uint32_t num_models, std::uint64_t const* seeds,
+                          std::uint32_t num_games, std::uint32_t max_moves, std::uint32_t threads, float* score_out,
+                          std::uint32_t* pieces_out, std::uint32_t* lines_out, std::uint64_t* evals_total) {
+    return eval_mt(play_wide_h<32>, wide_net<32>::P, w, num_models, seeds, num_games, max_moves, threads, score_out,
+                   pieces_out, lines_out, evals_total);
 }
 
 // Weights of ta3_gpu/tests/src/parity_test.cpp:20-32: mt19937{seed} with

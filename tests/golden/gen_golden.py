@@ -14,6 +14,7 @@ Outputs (committed; the tests read only these, never the reference):
                  the per-move (hold, orientation, x) trace and the final board
   wide.json      whole games of the widened 10 -> 64 -> 64 -> 1 network
                  (``python tests/golden/gen_golden.py wide`` regenerates only it)
+  wide32.json    games of the 10 -> 32 -> 32 -> 1 network (``... gen_golden.py wide32``)
 """
 from __future__ import annotations
 
@@ -205,9 +206,32 @@ def wide():
     return {"workload": b.name, "seeds": [str(int(x)) for x in b.seeds[0]], "max_moves": 300, "cases": cases}
 
 
+def wide32():
+    """The same for the 10 -> 32 -> 32 -> 1 network (ta3ref_eval_wide32_mt, one
+    thread): per game score, pieces and lines, and the batch's evaluated placements.
+    Weights as little-endian float32 hex (1,441 per model)."""
+    b = workload.wide_batch(islands=1, pop=6, games=3, max_moves=300, hidden=32)
+    seeds = np.ascontiguousarray(b.seeds[0], np.uint64)
+    w = np.ascontiguousarray(b.weights, np.float32)
+    n = b.models * seeds.size
+    sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    ev = C.c_uint64()
+    REF.ta3ref_eval_wide32_mt(ptr(w), b.models, ptr(seeds), seeds.size, 300, 1, ptr(sc), ptr(pc), ptr(lc),
+                              C.byref(ev))
+    cases = []
+    for m in range(b.models):
+        res = [{"seed": str(int(seeds[g])), "score": f32hex(sc[m * seeds.size + g]),
+                "pieces": int(pc[m * seeds.size + g]), "lines": int(lc[m * seeds.size + g])} for g in range(seeds.size)]
+        cases.append({"model": m, "weights_hex": w[m].astype("<f4").tobytes().hex(), "results": res})
+        print("wide32 model", m, [r["pieces"] for r in res], flush=True)
+    return {"workload": b.name, "seeds": [str(int(x)) for x in seeds], "max_moves": 300, "evals_total": ev.value,
+            "cases": cases}
+
+
 def main():
     only = sys.argv[1:]
-    for name, fn in (("tables", tables), ("engine", engine), ("boards", boards), ("games", games), ("wide", wide)):
+    for name, fn in (("tables", tables), ("engine", engine), ("boards", boards), ("games", games), ("wide", wide),
+                     ("wide32", wide32)):
         if only and name not in only:
             continue
         data = fn()

@@ -66,12 +66,12 @@ def test_v11_and_wide_share_a_context(ev):
     assert a.tobytes() == a2.tobytes() and v.shape == (2,)
 
 
-def _oracle_net(oracle, w, seeds, max_moves):
+def _oracle_net(oracle, w, seeds, max_moves, hidden=64):
     n = w.shape[0] * seeds.size
     osc, opc, olc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
     ev_total = C.c_uint64()
-    oracle.ta3o_eval_net_mt(ptr(w), 64, 64, w.shape[0], ptr(seeds), seeds.size, max_moves, 8, ptr(osc), ptr(opc),
-                            ptr(olc), C.byref(ev_total))
+    oracle.ta3o_eval_net_mt(ptr(w), hidden, hidden, w.shape[0], ptr(seeds), seeds.size, max_moves, 8, ptr(osc),
+                            ptr(opc), ptr(olc), C.byref(ev_total))
     return osc, opc, olc
 
 
@@ -133,3 +133,47 @@ def test_wide_time_budget_flavour(ev):
         ev.set_time_budget(0)
     again = ev.eval_full(w, w.shape[0], seeds, cap)
     assert all(x.tobytes() == y.tobytes() for x, y in zip(ref, again))
+
+
+def test_width32_matches_reference_games(ev):
+    """The 10 -> 32 -> 32 -> 1 instantiation against the reference's own games
+    (tests/golden/wide32.json): scores, pieces and lines bit-exact."""
+    g = load_golden("wide32")
+    w = np.stack([np.frombuffer(bytes.fromhex(c["weights_hex"]), "<f4") for c in g["cases"]]).astype(np.float32)
+    seeds = np.array([int(x) for x in g["seeds"]], np.uint64)
+    sc, pc, lc = ev.eval_full(w, w.shape[0], seeds, g["max_moves"])
+    for m, case in enumerate(g["cases"]):
+        for k, r in enumerate(case["results"]):
+            i = m * seeds.size + k
+            assert sc[i] == f32_from_hex(r["score"]) and pc[i] == r["pieces"] and lc[i] == r["lines"], (m, k)
+
+
+def test_width32_random_and_skipping_models_match_oracle(ev, oracle):
+    """Width 32 on further models: random initialisations, heavily sparse hidden
+    layers, and -0 biases (zero-term skipping off), against the oracle."""
+    from tetris_ai3_b200 import workload
+    b = workload.wide_batch(islands=1, pop=6, games=4, max_moves=150, seed=5, hidden=32)
+    w = b.weights.copy()
+    b1, b2 = slice(320, 352), slice(1376, 1408)         # [out][in] weights then biases, per layer
+    w[0, b1] = -0.75
+    w[1, b1] = np.float32(-0.0)
+    w[2, b2] = np.float32(-0.0)
+    w[3, 352:1376:3] = 0.0
+    seeds = np.ascontiguousarray(b.seeds[0])
+    sc, pc, lc = ev.eval_full(w, w.shape[0], seeds, b.max_moves)
+    osc, opc, olc = _oracle_net(oracle, w, seeds, b.max_moves, hidden=32)
+    assert sc.tobytes() == osc.tobytes()
+    assert np.array_equal(pc, opc) and np.array_equal(lc, olc)
+
+
+def test_width32_device_entry_matches_host_entry(ev):
+    import torch
+    from tetris_ai3_b200 import workload
+    b = workload.wide_batch(islands=1, pop=3, games=3, max_moves=80, seed=6, hidden=32)
+    host = ev.eval(b.weights, b.models, b.seeds[0], b.max_moves)
+    dev = torch.device("cuda", 0)
+    score = torch.zeros(b.sims, dtype=torch.float32, device=dev)
+    ev.eval_device(torch.from_numpy(b.weights).to(dev), torch.from_numpy(b.seeds.view(np.int64)).to(dev),
+                   b.max_moves, score)
+    torch.cuda.synchronize()
+    assert score.cpu().numpy().tobytes() == host.tobytes()

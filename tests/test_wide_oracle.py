@@ -57,3 +57,26 @@ def test_oracle_wide_trace_matches_reference(oracle, wide):
                          C.byref(e), tr, C.byref(nm), ptr(bd))
     assert nm.value == r["moves"] and bytes(tr)[:3 * nm.value].hex() == r["trace"] and bd.tolist() == r["board"]
     assert e.value == r["evals"]
+
+
+def test_oracle_matches_reference_width32_games(oracle):
+    """The 10 -> 32 -> 32 -> 1 network (tests/golden/wide32.json, made by the
+    reference harness's ta3ref_eval_wide32_mt): scores, pieces, lines, placements."""
+    from tetris_ai3_b200 import workload
+    g = load_golden("wide32")
+    assert oracle.ta3o_net_params(32, 32) == workload.NUM_PARAMS_WIDE32 == 1441
+    b = workload.wide_batch(islands=1, pop=len(g["cases"]), games=3, max_moves=300, hidden=32)
+    seeds = np.array([int(s) for s in g["seeds"]], np.uint64)
+    assert np.array_equal(seeds, b.seeds[0])
+    w = np.stack([np.frombuffer(bytes.fromhex(c["weights_hex"]), "<f4") for c in g["cases"]]).astype(np.float32)
+    assert np.array_equal(w, b.weights)
+    n = w.shape[0] * seeds.size
+    sc, pc, lc = np.zeros(n, np.float32), np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    ev = C.c_uint64()
+    assert oracle.ta3o_eval_net_mt(ptr(w), 32, 32, w.shape[0], ptr(seeds), seeds.size, g["max_moves"], 8, ptr(sc),
+                                   ptr(pc), ptr(lc), C.byref(ev)) == 0
+    for m, case in enumerate(g["cases"]):
+        for k, r in enumerate(case["results"]):
+            i = m * seeds.size + k
+            assert sc[i] == f32_from_hex(r["score"]) and pc[i] == r["pieces"] and lc[i] == r["lines"], (m, k)
+    assert ev.value == g["evals_total"]

@@ -224,27 +224,31 @@ TA3B_HD float value_full(uint32_t clear_bits, BoardInts const& bi, bool held_i, 
 
 // ---------------------------------------------- widened value network ---
 // The reference's dense layers (ta3_ai/incl/ta3/ai/models/models/utility.hpp:29-46)
-// widened: the v11 inputs -> 64 ReLU -> 64 ReLU -> 1, per layer [out][in]
-// weights then [out] biases (704 + 4160 + 65 = 4,929 parameters).
+// widened: the v11 inputs -> H ReLU -> H ReLU -> 1 for a compile-time width H, per
+// layer [out][in] weights then [out] biases (H = 64: 704 + 4160 + 65 = 4,929 parameters).
+template <int H>
+struct WideNet {
+    static constexpr int B1 = NIN * H, W2 = B1 + H, B2 = W2 + H * H, W3 = B2 + H, B3 = W3 + H, N = B3 + 1;
+    // Device copy (STRIDE floats, 16-byte aligned): the same offsets, but layers 1 and 2
+    // transposed to [in][out], so one input's weights to all H units are contiguous; the
+    // word after the last bias is SKIP (the zero-term flag).
+    static constexpr int W1T = 0, W2T = W2, SKIP = N, STRIDE = (N + 1 + 3) / 4 * 4;
+    static_assert(H % 4 == 0 && B1 % 4 == 0 && W2 % 4 == 0 && B2 % 4 == 0 && W3 % 4 == 0 && STRIDE > SKIP,
+                  "16-byte aligned blocks");
+    // device-layout index of parameter j (reference order)
+    static TA3B_HD int device_index(int j) {
+        if (j < B1) return W1T + (j % NIN) * H + j / NIN;
+        if (j >= W2 && j < B2) return W2T + ((j - W2) % H) * H + (j - W2) / H;
+        return j;
+    }
+    static TA3B_HD bool is_bias(int j) { return (j >= B1 && j < W2) || (j >= B2 && j < W3) || j == B3; }
+};
+// the widths the kernels are built for: 64 (configs[4]'s 4,929 parameters) and 32 (1,441)
 constexpr int WH = 64;
-constexpr int WIDE_B1 = NIN * WH, WIDE_W2 = WIDE_B1 + WH, WIDE_B2 = WIDE_W2 + WH * WH, WIDE_W3 = WIDE_B2 + WH,
-              WIDE_B3 = WIDE_W3 + WH, NPARAMS_WIDE = WIDE_B3 + 1;
-static_assert(NPARAMS_WIDE == 4929, "10 -> 64 -> 64 -> 1");
-// Device copy of a widened model (WIDE_STRIDE floats, 16-byte aligned): the same
-// offsets, but layers 1 and 2 transposed to [in][out], so one input's weights to all
-// 64 units are contiguous; the word after the last bias is WIDE_SKIP (below).
-constexpr int WIDE_W1T = 0, WIDE_W2T = WIDE_W2, WIDE_SKIP = NPARAMS_WIDE, WIDE_STRIDE = 4932;
-static_assert(WIDE_STRIDE % 4 == 0 && WIDE_STRIDE > WIDE_SKIP && WIDE_B1 % 4 == 0 && WIDE_W2 % 4 == 0 &&
-                  WIDE_B2 % 4 == 0 && WIDE_W3 % 4 == 0 && WH % 4 == 0, "16-byte aligned blocks");
-// Device-layout index of parameter j of a widened model (reference order).
-TA3B_HD int wide_device_index(int j) {
-    if (j < WIDE_B1) return WIDE_W1T + (j % NIN) * WH + j / NIN;
-    if (j >= WIDE_W2 && j < WIDE_B2) return WIDE_W2T + ((j - WIDE_W2) % WH) * WH + (j - WIDE_W2) / WH;
-    return j;
-}
-TA3B_HD bool wide_is_bias(int j) {
-    return (j >= WIDE_B1 && j < WIDE_W2) || (j >= WIDE_B2 && j < WIDE_W3) || j == WIDE_B3;
-}
+using Wide64 = WideNet<64>;
+using Wide32 = WideNet<32>;
+constexpr int NPARAMS_WIDE = Wide64::N, NPARAMS_WIDE32 = Wide32::N;
+static_assert(NPARAMS_WIDE == 4929 && NPARAMS_WIDE32 == 1441 && Wide64::STRIDE == 4932, "10 -> H -> H -> 1");
 
 TA3B_HD float relu(float v) { return v > 0.0f ? v : 0.0f; }    // std::max<float>(0, v)
 

@@ -253,14 +253,18 @@ __device__ __forceinline__ int fast_candidate(uint32_t const* __restrict__ rec, 
 struct WideIn {
     float v[NIN];
 };
-constexpr int WIDE_HB_FLOATS = WH * WARP;              // per warp: 64 units x 32 lanes (8 KB)
+template <int H>
+constexpr int kWideHbFloats = H * WARP;                // per warp: H units x 32 lanes (8 KB for 64)
 
+template <int H>
 __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w, float* __restrict__ hb, int lane) {
-    uint32_t const skip = __ldg(reinterpret_cast<uint32_t const*>(w) + WIDE_SKIP);
-    float a[WH];
+    static_assert(H >= 4 && H <= 64 && H % 4 == 0, "the hidden-unit masks hold 64 units");
+    using D = WideNet<H>;
+    uint32_t const skip = __ldg(reinterpret_cast<uint32_t const*>(w) + D::SKIP);
+    float a[H];
 #pragma unroll
-    for (int o = 0; o < WH; o += 4) {
-        float4 const b = __ldg(reinterpret_cast<float4 const*>(w + WIDE_B1 + o));
+    for (int o = 0; o < H; o += 4) {
+        float4 const b = __ldg(reinterpret_cast<float4 const*>(w + D::B1 + o));
         a[o] = b.x; a[o + 1] = b.y; a[o + 2] = b.z; a[o + 3] = b.w;
     }
     // layer 1, one input at a time over all 64 units (inputs that are zero in every lane skipped)
@@ -271,10 +275,10 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
 #pragma unroll
     for (int i = 0; i < NIN; ++i) {
         if (!((inz >> i) & 1u)) continue;
-        float4 const* wr = reinterpret_cast<float4 const*>(w + WIDE_W1T + i * WH);
+        float4 const* wr = reinterpret_cast<float4 const*>(w + D::W1T + i * H);
         float const x = in.v[i];
 #pragma unroll
-        for (int o = 0; o < WH; o += 4) {
+        for (int o = 0; o < H; o += 4) {
             float4 const q = __ldg(wr + o / 4);
             a[o] = f_add(a[o], f_mul(x, q.x));
             a[o + 1] = f_add(a[o + 1], f_mul(x, q.y));
@@ -285,7 +289,7 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
     // ReLU into the buffer; nz = the units that are non-zero in some lane
     uint32_t nz[2] = {0u, 0u};
 #pragma unroll
-    for (int o = 0; o < WH; o += 4) {
+    for (int o = 0; o < H; o += 4) {
         float4 const h = make_float4(relu(a[o]), relu(a[o + 1]), relu(a[o + 2]), relu(a[o + 3]));
         float* const hq = hb + lane;
         hq[(o + 0) * WARP] = h.x;
@@ -304,19 +308,20 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
     }
     // layer 2, one hidden unit at a time over all 64 outputs
 #pragma unroll
-    for (int o = 0; o < WH; o += 4) {
-        float4 const b = __ldg(reinterpret_cast<float4 const*>(w + WIDE_B2 + o));
+    for (int o = 0; o < H; o += 4) {
+        float4 const b = __ldg(reinterpret_cast<float4 const*>(w + D::B2 + o));
         a[o] = b.x; a[o + 1] = b.y; a[o + 2] = b.z; a[o + 3] = b.w;
     }
     float const* hs = hb + lane;
     uint64_t m = (uint64_t(nz[1]) << 32) | nz[0];
+    if (H < 64) m &= (uint64_t(1) << (H & 63)) - 1u;         // only the H units that exist
     while (m) {
         int const i = __ffsll(static_cast<long long>(m)) - 1;
         m &= m - 1;
         float const x = hs[i * WARP];
-        float4 const* wr = reinterpret_cast<float4 const*>(w + WIDE_W2T + i * WH);
+        float4 const* wr = reinterpret_cast<float4 const*>(w + D::W2T + i * H);
 #pragma unroll
-        for (int o = 0; o < WH; o += 4) {
+        for (int o = 0; o < H; o += 4) {
             float4 const q = __ldg(wr + o / 4);
             a[o] = f_add(a[o], f_mul(x, q.x));
             a[o + 1] = f_add(a[o + 1], f_mul(x, q.y));
@@ -325,10 +330,10 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
         }
     }
     // layer 3: every term, ascending
-    float out = __ldg(w + WIDE_B3);
+    float out = __ldg(w + D::B3);
 #pragma unroll
-    for (int o = 0; o < WH; o += 4) {
-        float4 const q = __ldg(reinterpret_cast<float4 const*>(w + WIDE_W3 + o));
+    for (int o = 0; o < H; o += 4) {
+        float4 const q = __ldg(reinterpret_cast<float4 const*>(w + D::W3 + o));
         out = f_add(out, f_mul(relu(a[o]), q.x));
         out = f_add(out, f_mul(relu(a[o + 1]), q.y));
         out = f_add(out, f_mul(relu(a[o + 2]), q.z));
@@ -338,6 +343,7 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
 }
 
 // fast path of the widened network: the same record words; every lane of the warp calls it
+template <int H>
 __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ rec, PlaceFast pf, bool held_i,
                                                    float const* __restrict__ w, float* hb, int lane, float& v) {
     RecView r;
@@ -348,7 +354,7 @@ __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ 
     r.combo = rec[R_COMBO + ((pf.m >> 16) & 63u)];
     WideIn in;
     bool const defer = fast_wide_inputs(r, rec[R_CLEARS], pf, held_i, in.v);
-    v = wide_value(in, w, hb, lane);
+    v = wide_value<H>(in, w, hb, lane);
     return defer ? FAST_DEFER : FAST_OK;
 }
 
@@ -506,9 +512,11 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality.
-template <bool WIDE>
+template <int NET>
 __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float* hb, bool leaf,
                                                uint32_t total, int kl, int lane, uint32_t& evals) {
+    constexpr bool WIDE = NET != 0;
+    constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
     LevelAcc acc{0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
@@ -535,7 +543,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
                 if (!legal) in = WideIn{};
             }
             __syncwarp();
-            float const v = wide_value(in, ws.wglobal, hb, lane);
+            float const v = wide_value<HW>(in, ws.wglobal, hb, lane);
             if (legal) {
                 uint32_t const info = ws.seg_info[entry >> 8];
                 key = candidate_key(leaf, v, info, entry & 0xFFu);
@@ -578,9 +586,9 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
         int st[TA3B_ILP];
 #pragma unroll
         for (int u = 0; u < TA3B_ILP; ++u) {
-            if (WIDE)
-                st[u] = fast_candidate_wide(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
-                                            (info[u] >> 20) & 1u, ws.wglobal, hb, lane, v[u]);
+            if constexpr (WIDE)
+                st[u] = fast_candidate_wide<HW>(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
+                                                (info[u] >> 20) & 1u, ws.wglobal, hb, lane, v[u]);
             else
                 st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
                                        (info[u] >> 20) & 1u, fw, v[u]);
@@ -677,9 +685,10 @@ __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
 }
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
-template <bool WIDE>
+template <int NET>
 __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
+    constexpr bool WIDE = NET != 0;
     Move mv{0, 0, 0, true};
     if (ws.eng.over) return mv;
     uint32_t slot_piece[NSLOTS];                                  // beam.hpp:226-237
@@ -719,7 +728,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
         // ---- every candidate of the stage
-        LevelAcc const a = level_pass<WIDE>(ws, lut, fw, hb, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2),
+        LevelAcc const a = level_pass<NET>(ws, lut, fw, hb, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2),
                                              lane, evals);
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
@@ -788,11 +797,14 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     return mv;
 }
 
-// WIDE: the widened 10 -> 64 -> 64 -> 1 network (4,929 weights per model) instead of v11.
+// NET: 0 = the v11 model; H = the widened 10 -> H -> H -> 1 network (64: 4,929 weights per
+// model, 32: 1,441) instead of v11.
 // BUDGET: the flavour that checks the launch's time budget after every move (a separate
 // instantiation: the check's registers would otherwise cost the ordinary kernels spills).
-template <int WARPS, int MINB, bool WIDE = false, bool BUDGET = false>
+template <int WARPS, int MINB, int NET = 0, bool BUDGET = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
+    constexpr bool WIDE = NET != 0;
+    constexpr int HW = WIDE ? NET : 64;
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
     for (int t = int(threadIdx.x); t < NPIECE * MP; t += WARPS * 32) {
@@ -805,7 +817,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
     // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
     float* const hb = WIDE ? reinterpret_cast<float*>(dyn_smem + WARPS * sizeof(WarpShared)) +
-                                 (threadIdx.x >> 5) * WIDE_HB_FLOATS
+                                 (threadIdx.x >> 5) * kWideHbFloats<HW>
                            : nullptr;
     // time budget, measured from this warp's start (the persistent grid starts every warp at launch);
     // kept in shared memory so it costs no register in the move loop
@@ -818,7 +830,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
-        float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WIDE_STRIDE : NPARAMS);
+        float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WideNet<HW>::STRIDE : NPARAMS);
         if (p.timing && lane == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -837,7 +849,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         __syncwarp();
         uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move<WIDE>(ws, lut, fw, hb, lane, evals, &p.scratch[1]);
+            Move const mv = search_move<NET>(ws, lut, fw, hb, lane, evals, &p.scratch[1]);
             if (mv.none) break;
             if (lane == 0) {
                 if (p.trace) {
@@ -916,22 +928,24 @@ __global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand,
     full_v[t] = full_legal[t] ? value_full(rec[R_CLEARS] + clear_bump(cl), board_ints(nb), held, GlobalW{w}) : 0.0f;
 }
 
-// widened models -> their device layout (WIDE_STRIDE floats per model: layers 1
-// and 2 transposed, WIDE_SKIP = 1 when zero terms may be left out). One block per model.
+// widened models -> their device layout (WideNet<H>::STRIDE floats per model: layers
+// 1 and 2 transposed, SKIP = 1 when zero terms may be left out). One block per model.
+template <int H>
 __global__ void repack_wide_kernel(float const* __restrict__ src, uint32_t models, float* __restrict__ dst) {
+    using D = WideNet<H>;
     uint32_t const m = blockIdx.x;
     if (m >= models) return;
-    float const* s = src + size_t(m) * NPARAMS_WIDE;
-    float* d = dst + size_t(m) * WIDE_STRIDE;
+    float const* s = src + size_t(m) * D::N;
+    float* d = dst + size_t(m) * D::STRIDE;
     int ok = 1;
-    for (int j = int(threadIdx.x); j < NPARAMS_WIDE; j += int(blockDim.x)) {
+    for (int j = int(threadIdx.x); j < D::N; j += int(blockDim.x)) {
         float const x = s[j];
-        ok &= isfinite(x) && !(wide_is_bias(j) && x == 0.0f && signbit(x));
-        d[wide_device_index(j)] = x;
+        ok &= isfinite(x) && !(D::is_bias(j) && x == 0.0f && signbit(x));
+        d[D::device_index(j)] = x;
     }
     ok = __syncthreads_and(ok);
-    if (threadIdx.x < uint32_t(WIDE_STRIDE - WIDE_SKIP))
-        reinterpret_cast<uint32_t*>(d)[WIDE_SKIP + threadIdx.x] = threadIdx.x == 0 && ok ? 1u : 0u;
+    if (threadIdx.x < uint32_t(D::STRIDE - D::SKIP))
+        reinterpret_cast<uint32_t*>(d)[D::SKIP + threadIdx.x] = threadIdx.x == 0 && ok ? 1u : 0u;
 }
 constexpr uint32_t kRepackThreads = 256;
 
@@ -951,16 +965,17 @@ Variant const kVariants[] = {
     {eval_kernel<10, 2>, 10, 2}, {eval_kernel<20, 1>, 20, 1},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
+// the networks a launch can run: v11, or the widened 10 -> H -> H -> 1 for H = 64 or 32
+enum NetKind { NET_V11 = 0, NET_W64 = 1, NET_W32 = 2, NUM_NETS = 3 };
+constexpr int net_width(int ni) { return ni == NET_W64 ? 64 : ni == NET_W32 ? 32 : 0; }
 // dynamic shared memory per warp: its WarpShared block, plus the widened network's hidden-unit buffer
-constexpr size_t warp_bytes(bool wide) { return sizeof(WarpShared) + (wide ? WIDE_HB_FLOATS * sizeof(float) : 0); }
-// the widened network: ~10,000 FP32 operations per candidate, more registers per lane
-Variant const kWideVariants[] = {
-    {eval_kernel<4, 2, true>, 4, 2}, {eval_kernel<4, 3, true>, 4, 3}, {eval_kernel<4, 4, true>, 4, 4},
-};
-constexpr int kDefaultWideVariant = 0;
+constexpr size_t warp_bytes(int ni) { return sizeof(WarpShared) + size_t(net_width(ni)) * WARP * sizeof(float); }
+// the widened networks' launch shapes (more registers per lane than v11): width 64 at 2 blocks
+// of 4 warps per SM (255 registers), width 32 at 3
+Variant const kWideNet[NUM_NETS] = {{nullptr, 0, 0}, {eval_kernel<4, 2, 64>, 4, 2}, {eval_kernel<4, 3, 32>, 4, 3}};
 // the budget-checking flavours (shapes where the extra check spills nothing)
-Variant const kBudgetV11 = {eval_kernel<4, 3, false, true>, 4, 3};
-Variant const kBudgetWide = {eval_kernel<4, 2, true, true>, 4, 2};
+Variant const kBudgetNet[NUM_NETS] = {{eval_kernel<4, 3, 0, true>, 4, 3}, {eval_kernel<4, 2, 64, true>, 4, 2},
+                                      {eval_kernel<4, 3, 32, true>, 4, 3}};
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
@@ -998,9 +1013,8 @@ struct ta3b_ctx {
     float* d_wpad = nullptr;          // widened models in their padded device layout
     size_t cap_wpad = 0;
     unsigned long long budget_ns = 0; // per-launch time budget (0 = none)
-    int wide_variant = -1;            // widened-network kernel, set up on first use
-    uint32_t budget_grid[2] = {0, 0};  // budget flavours (v11, widened), set up on first use
-    uint32_t wide_warps = 0, wide_grid = 0;
+    uint32_t net_grid[NUM_NETS] = {0, 0, 0};     // widened-network kernels (by NetKind), set up on first use
+    uint32_t budget_grid[NUM_NETS] = {0, 0, 0};  // budget flavours (by NetKind), set up on first use
     uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
     std::string err;
 };
@@ -1036,12 +1050,30 @@ int grow(ta3b_ctx* ctx, T*& ptr, size_t& cap, size_t need, char const* what) {
     return TA3B_OK;
 }
 
+// the network a parameter count selects
+int net_of(uint32_t num_params) {
+    return num_params == uint32_t(NPARAMS_WIDE) ? NET_W64 : num_params == uint32_t(NPARAMS_WIDE32) ? NET_W32 : NET_V11;
+}
+uint32_t net_stride(int ni) { return ni == NET_W64 ? Wide64::STRIDE : ni == NET_W32 ? Wide32::STRIDE : NPARAMS; }
+
+// widened models -> their device layout in ctx->d_wpad (grown to fit), on `st`
+int repack_models(ta3b_ctx* ctx, int ni, float const* d_src, uint64_t models, cudaStream_t st) {
+    if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * net_stride(ni), "alloc padded weights")) return rc;
+    if (ni == NET_W64)
+        repack_wide_kernel<64><<<uint32_t(models), kRepackThreads, 0, st>>>(d_src, uint32_t(models), ctx->d_wpad);
+    else
+        repack_wide_kernel<32><<<uint32_t(models), kRepackThreads, 0, st>>>(d_src, uint32_t(models), ctx->d_wpad);
+    TA3B_CUDA(ctx, cudaGetLastError(), "repack widened weights");
+    return TA3B_OK;
+}
+
 int check_sizes(ta3b_ctx* ctx, uint32_t num_islands, uint32_t models_per_island, uint32_t num_params,
                 uint32_t num_games) {
     if (!ctx) return fail(ctx, TA3B_ERR_ARG, "null context");
-    if (num_params != NPARAMS && num_params != NPARAMS_WIDE)
-        return fail(ctx, TA3B_ERR_ARG, "num_params must be " + std::to_string(NPARAMS) + " (v11) or " +
-                                           std::to_string(NPARAMS_WIDE) + " (10 -> 64 -> 64 -> 1)");
+    if (num_params != NPARAMS && num_params != uint32_t(NPARAMS_WIDE) && num_params != uint32_t(NPARAMS_WIDE32))
+        return fail(ctx, TA3B_ERR_ARG, "num_params must be " + std::to_string(NPARAMS) + " (v11), " +
+                                           std::to_string(NPARAMS_WIDE) + " (10 -> 64 -> 64 -> 1) or " +
+                                           std::to_string(NPARAMS_WIDE32) + " (10 -> 32 -> 32 -> 1)");
     uint64_t const sims = uint64_t(num_islands) * models_per_island * num_games;
     if (sims > 0xFFFFFFF0ull) return fail(ctx, TA3B_ERR_ARG, "too many sims in one batch");
     return TA3B_OK;
@@ -1067,32 +1099,11 @@ int set_min_carveout(ta3b_ctx* ctx, Variant const& v, size_t dyn) {
     return TA3B_OK;
 }
 
-int setup_wide(ta3b_ctx* ctx) {
-    if (ctx->wide_variant >= 0) return TA3B_OK;
-    Variant const& v = kWideVariants[kDefaultWideVariant];
-    size_t const dyn = v.warps * warp_bytes(true);
+// shared-memory limits, carveout and resident grid of one widened or budget kernel
+int setup_kernel(ta3b_ctx* ctx, Variant const& v, int ni, uint32_t& grid_out, char const* what) {
+    size_t const dyn = v.warps * warp_bytes(ni);
     TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
-    if (int rc = set_min_carveout(ctx, v, dyn)) return rc;
-    int per_sm = 0;
-    TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
-    if (per_sm < int(v.min_blocks)) {   // the split chosen leaves too little shared memory: take the maximum
-        TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                            cudaSharedmemCarveoutMaxShared), "smem carveout");
-        TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
-    }
-    if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "widened kernel does not fit on an SM");
-    ctx->wide_variant = kDefaultWideVariant;
-    ctx->wide_warps = v.warps;
-    ctx->wide_grid = ctx->sms * uint32_t(per_sm);
-    return TA3B_OK;
-}
-
-int setup_budget(ta3b_ctx* ctx, bool wide) {
-    if (ctx->budget_grid[wide]) return TA3B_OK;
-    Variant const& v = wide ? kBudgetWide : kBudgetV11;
-    size_t const dyn = v.warps * warp_bytes(wide);
-    TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn)), "dynamic smem size");
-    if (wide) {
+    if (ni != NET_V11) {
         if (int rc = set_min_carveout(ctx, v, dyn)) return rc;
     } else {
         TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
@@ -1100,34 +1111,33 @@ int setup_budget(ta3b_ctx* ctx, bool wide) {
     }
     int per_sm = 0;
     TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
-    if (wide && per_sm < int(v.min_blocks)) {
+    if (ni != NET_V11 && per_sm < int(v.min_blocks)) {   // the split chosen leaves too little shared memory
         TA3B_CUDA(ctx, cudaFuncSetAttribute(v.fn, cudaFuncAttributePreferredSharedMemoryCarveout,
                                             cudaSharedmemCarveoutMaxShared), "smem carveout");
         TA3B_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn, v.warps * 32, dyn), "occupancy");
     }
-    if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "budget kernel does not fit on an SM");
-    ctx->budget_grid[wide] = ctx->sms * uint32_t(per_sm);
+    if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, std::string(what) + " does not fit on an SM");
+    grid_out = ctx->sms * uint32_t(per_sm);
     return TA3B_OK;
 }
 
-int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, bool wide = false) {
+int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) {
     if (prm.total_sims == 0) return TA3B_OK;
-    if (wide)
-        if (int rc = setup_wide(ctx)) return rc;
+    if (ni != NET_V11 && !ctx->net_grid[ni])
+        if (int rc = setup_kernel(ctx, kWideNet[ni], ni, ctx->net_grid[ni], "widened kernel")) return rc;
     bool const budget = ctx->budget_ns != 0;
-    if (budget)
-        if (int rc = setup_budget(ctx, wide)) return rc;
+    if (budget && !ctx->budget_grid[ni])
+        if (int rc = setup_kernel(ctx, kBudgetNet[ni], ni, ctx->budget_grid[ni], "budget kernel")) return rc;
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, 2 * sizeof(uint32_t), st), "reset work queue");
     // with a time budget the budget-checking flavour runs (its own fixed launch shape)
-    Variant const* bv = budget ? (wide ? &kBudgetWide : &kBudgetV11) : nullptr;
-    uint32_t const warps = bv ? bv->warps : wide ? ctx->wide_warps : ctx->warps_per_block;
-    uint32_t const max_grid = bv ? ctx->budget_grid[wide] : wide ? ctx->wide_grid : ctx->grid;
+    Variant const* const v = budget ? &kBudgetNet[ni] : ni != NET_V11 ? &kWideNet[ni] : &kVariants[ctx->variant];
+    uint32_t const warps = v->warps;
+    uint32_t const max_grid = budget ? ctx->budget_grid[ni] : ni != NET_V11 ? ctx->net_grid[ni] : ctx->grid;
     uint32_t const need_blocks = (prm.total_sims + warps - 1) / warps;
     uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
-    KernelFn const fn = bv ? bv->fn : wide ? kWideVariants[ctx->wide_variant].fn : kVariants[ctx->variant].fn;
     Params p2 = prm;
     p2.budget_ns = ctx->budget_ns;
-    fn<<<grid, warps * 32, warps * warp_bytes(wide), st>>>(p2);
+    v->fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     ctx->last_grid = grid;
     ctx->last_warps = warps;
@@ -1181,13 +1191,12 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
             ctx->cap_tb = sims;
         }
     }
-    bool const wide = num_params == NPARAMS_WIDE;
+    int const ni = net_of(num_params);
+    bool const wide = ni != NET_V11;
     if (wide) {   // the models as given (d_w), then their device layout (d_wpad)
-        if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * WIDE_STRIDE, "alloc padded weights")) return rc;
         TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float), cudaMemcpyHostToDevice,
                                        ctx->stream), "copy weights");
-        repack_wide_kernel<<<uint32_t(models), kRepackThreads, 0, ctx->stream>>>(ctx->d_w, uint32_t(models), ctx->d_wpad);
-        TA3B_CUDA(ctx, cudaGetLastError(), "repack widened weights");
+        if (int rc = repack_models(ctx, ni, ctx->d_w, models, ctx->stream)) return rc;
     } else {
         TA3B_CUDA(ctx, cudaMemcpyAsync(ctx->d_w, weights, models * num_params * sizeof(float),
                                        cudaMemcpyHostToDevice, ctx->stream), "copy weights");
@@ -1210,7 +1219,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     prm.models_per_island = mpi;
     prm.max_moves = max_moves;
     prm.total_sims = uint32_t(sims);
-    if (int rc = launch(ctx, prm, ctx->stream, num_params == NPARAMS_WIDE)) return rc;
+    if (int rc = launch(ctx, prm, ctx->stream, ni)) return rc;
     TA3B_CUDA(ctx, cudaMemcpyAsync(score_out, ctx->d_score, sims * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
               "copy score");
     if (pieces_out)
@@ -1364,13 +1373,10 @@ int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands
     if (sims == 0) return TA3B_OK;
     if (!d_weights || !d_seeds || !d_score) return fail(ctx, TA3B_ERR_ARG, "null device pointer");
     cudaStream_t const st = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
-    bool const wide = num_params == NPARAMS_WIDE;
-    if (wide) {   // the padded copy (allocated on the first widened call of this size)
-        uint64_t const models = uint64_t(num_islands) * models_per_island;
-        if (int rc = grow(ctx, ctx->d_wpad, ctx->cap_wpad, models * WIDE_STRIDE, "alloc padded weights")) return rc;
-        repack_wide_kernel<<<uint32_t(models), kRepackThreads, 0, st>>>(d_weights, uint32_t(models), ctx->d_wpad);
-        TA3B_CUDA(ctx, cudaGetLastError(), "repack widened weights");
-    }
+    int const ni = net_of(num_params);
+    bool const wide = ni != NET_V11;
+    if (wide)   // the padded copy (allocated on the first widened call of this size)
+        if (int rc = repack_models(ctx, ni, d_weights, uint64_t(num_islands) * models_per_island, st)) return rc;
     Params prm{};
     prm.weights = wide ? ctx->d_wpad : d_weights;
     prm.seeds = d_seeds;
@@ -1383,7 +1389,7 @@ int ta3b_eval_device(ta3b_ctx* ctx, float const* d_weights, uint32_t num_islands
     prm.models_per_island = models_per_island;
     prm.max_moves = max_moves;
     prm.total_sims = uint32_t(sims);
-    return launch(ctx, prm, st, wide);
+    return launch(ctx, prm, st, ni);
 }
 
 int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out) {

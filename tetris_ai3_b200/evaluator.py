@@ -15,9 +15,10 @@ import os
 
 import numpy as np
 
-from .workload import NUM_PARAMS, NUM_PARAMS_WIDE
+from .workload import NUM_PARAMS, NUM_PARAMS_WIDE, NUM_PARAMS_WIDE32
 
-MODEL_SIZES = (NUM_PARAMS, NUM_PARAMS_WIDE)   # v11 (10 -> 8 -> 1), widened (10 -> 64 -> 64 -> 1)
+# v11 (10 -> 8 -> 1), widened (10 -> 64 -> 64 -> 1, 10 -> 32 -> 32 -> 1)
+MODEL_SIZES = (NUM_PARAMS, NUM_PARAMS_WIDE, NUM_PARAMS_WIDE32)
 
 
 def _rows(weights) -> np.ndarray:

@@ -22,10 +22,21 @@ import os
 import numpy as np
 
 NUM_PARAMS = 97          # ta3_ai/incl/ta3/ai/models/models/model_v11.hpp:44
-# the reference's dense layers widened to 10 -> 64 -> 64 -> 1 (utility.hpp:29-46 layout per layer:
-# [out][in] weights then [out] biases)
-WIDE_LAYERS = ((10, 64), (64, 64), (64, 1))
-NUM_PARAMS_WIDE = sum(i * o + o for i, o in WIDE_LAYERS)   # 4929
+# the reference's dense layers widened to 10 -> H -> H -> 1 (utility.hpp:29-46 layout per layer:
+# [out][in] weights then [out] biases); the kernels are built for H = 64 and H = 32
+
+
+def wide_layers(hidden: int = 64):
+    return ((10, hidden), (hidden, hidden), (hidden, 1))
+
+
+def wide_params(hidden: int = 64) -> int:
+    return sum(i * o + o for i, o in wide_layers(hidden))
+
+
+WIDE_LAYERS = wide_layers(64)
+NUM_PARAMS_WIDE = wide_params(64)        # 4929
+NUM_PARAMS_WIDE32 = wide_params(32)      # 1441
 _GOLDEN = np.uint64(0x9E3779B97F4A7C15)
 _M64 = (1 << 64) - 1
 
@@ -154,23 +165,25 @@ def uneven_batch(models: int = 200, games: int = 100, max_moves: int = 10000, se
     return Batch(f"{models} models x {games} games (10% champion), cap {max_moves}", w[order], seeds, max_moves)
 
 
-def wide_scale() -> np.ndarray:
+def wide_scale(hidden: int = 64) -> np.ndarray:
     """Per-parameter standard deviation of the widened network's initialisation:
     1 / sqrt(fan_in) for weights, 0 for biases."""
     parts = []
-    for fan_in, fan_out in WIDE_LAYERS:
+    for fan_in, fan_out in wide_layers(hidden):
         parts.append(np.full(fan_in * fan_out, 1.0 / np.sqrt(fan_in)))
         parts.append(np.zeros(fan_out))
     return np.concatenate(parts)
 
 
-def wide_batch(islands: int = 8, pop: int = 100, games: int = 100, max_moves: int = 2000, seed: int = 3) -> Batch:
-    """The widened evaluator's generation: islands x pop models of the 10 -> 64 ->
-    64 -> 1 network, each an independent N(0, 1/fan_in) initialisation drawn from
+def wide_batch(islands: int = 8, pop: int = 100, games: int = 100, max_moves: int = 2000, seed: int = 3,
+               hidden: int = 64) -> Batch:
+    """The widened evaluator's generation: islands x pop models of the 10 -> hidden ->
+    hidden -> 1 network, each an independent N(0, 1/fan_in) initialisation drawn from
     ``seed``; island i plays the ``games`` seeds simulate() derives from seed*1000+i."""
-    z = normal(seed, islands * pop * NUM_PARAMS_WIDE).reshape(islands * pop, NUM_PARAMS_WIDE)
-    sc = wide_scale()
+    n = wide_params(hidden)
+    z = normal(seed, islands * pop * n).reshape(islands * pop, n)
+    sc = wide_scale(hidden)
     w = np.where(sc[None, :] > 0, z * sc[None, :], 0.0).astype(np.float32)   # biases exactly +0
     seeds = np.stack([xoshiro_seeds(seed * 1000 + i, games) for i in range(islands)])
-    return Batch(f"widened 10-64-64-1: {islands} islands x {pop} x {games} games = {islands * pop * games} sims, "
-                 f"cap {max_moves}", w, seeds, max_moves)
+    return Batch(f"widened 10-{hidden}-{hidden}-1: {islands} islands x {pop} x {games} games = "
+                 f"{islands * pop * games} sims, cap {max_moves}", w, seeds, max_moves)
