@@ -60,7 +60,8 @@ int ta3s_predict(ta3s_model* m, const float* x, uint32_t n, float* mean_out, flo
  * to a multiple of 128:
  *   W1 [H][INP] (columns in_dim.. are zero padding), W2 [H][H], W3 [2][H],
  *   b1 [H], b2 [H], b3 [2]. Gradients use the same layout.
- * Calls mirror the ta3s_* functions above. A model is not thread-safe. */
+ * Calls mirror the ta3s_* functions above; ta3w_gradients takes at most 65,536
+ * rows and ta3w_train a minibatch of at most 65,536. A model is not thread-safe. */
 typedef struct ta3w_model ta3w_model;
 
 uint32_t ta3w_num_params(uint32_t in_dim, uint32_t hidden);   /* 0 for unsupported sizes */

@@ -143,3 +143,11 @@ def test_prescreening_gains_over_choosing_without_it(shape):
     without = true[:50].mean()              # what plain evaluation of 50 samples would keep
     spread = true.std()
     assert picked - without > 0.3 * spread, (picked, without, spread)
+
+
+def test_oversized_passes_are_rejected(sur):
+    from tetris_ai3_b200 import EvaluatorError
+    x = np.zeros((4, WIDE[0]), np.float32)
+    y = np.zeros(4, np.float32)
+    with pytest.raises(EvaluatorError, match="65,536"):
+        sur.train(x, y, epochs=1, batch=70000)

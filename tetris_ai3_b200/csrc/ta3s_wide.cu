@@ -469,6 +469,9 @@ int walloc(ta3w_model* m, T*& ptr, size_t n, char const* what) {
 }
 
 int round128(int n) { return (n + TILE - 1) / TILE * TILE; }
+// rows of one forward / backward pass: bounds the activation buffers (split-K partials
+// of the first layer alone take splits x rows x H floats)
+constexpr uint32_t kMaxPassRows = 65536;
 
 // activation buffers for `rows` (a multiple of 128) rows
 int ensure_act(ta3w_model* m, size_t rows) {
@@ -742,6 +745,7 @@ int ta3w_set_data_standardized(ta3w_model* m, const float* x, const float* y, ui
 int ta3w_gradients(ta3w_model* m, float* grad_out, float* loss_sum_out) {
     if (!m || !grad_out) return wfail(m, "ta3w_gradients: null argument");
     if (m->rows == 0) return wfail(m, "ta3w_gradients: no data");
+    if (m->rows > kMaxPassRows) return wfail(m, "ta3w_gradients: at most 65,536 rows in one pass");
     TA3W_CUDA(m, cudaSetDevice(m->device), "set device");
     TA3W_CUDA(m, cudaMemsetAsync(m->d_status, 0, 4, m->stream), "status");
     TA3W_CUDA(m, cudaMemsetAsync(m->d_grad, 0, size_t(m->d.n) * 4, m->stream), "grad");
@@ -754,7 +758,7 @@ int ta3w_gradients(ta3w_model* m, float* grad_out, float* loss_sum_out) {
 
 int ta3w_train(ta3w_model* m, uint32_t epochs, uint32_t batch, float lr, float weight_decay, uint32_t seed,
                float* final_loss) {
-    if (!m || batch == 0) return wfail(m, "ta3w_train: batch must be positive");
+    if (!m || batch == 0 || batch > kMaxPassRows) return wfail(m, "ta3w_train: batch must be 1 .. 65,536");
     if (m->rows == 0) return wfail(m, "ta3w_train: no data");
     TA3W_CUDA(m, cudaSetDevice(m->device), "set device");
     Dims const& d = m->d;
