@@ -243,7 +243,7 @@ struct WideNet {
     }
     static TA3B_HD bool is_bias(int j) { return (j >= B1 && j < W2) || (j >= B2 && j < W3) || j == B3; }
 };
-// the widths the kernels are built for: 64 (configs[4]'s 4,929 parameters) and 32 (1,441)
+// the widths the kernels are built for: 64 (4,929 parameters, the 80k-sim widened generation) and 32 (1,441)
 constexpr int WH = 64;
 using Wide64 = WideNet<64>;
 using Wide32 = WideNet<32>;
