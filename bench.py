@@ -48,10 +48,16 @@ REF_OPS_PER_PLACEMENT = 1010
 # The widened 10 -> 64 -> 64 -> 1 network replaces the MLP's 192 by
 # 64 x (10 mul + 10 add + relu) + 64 x (64 mul + 64 add + relu) + 64 mul + 64 add = 9,728.
 REF_OPS_PER_PLACEMENT_WIDE = 1010 - 192 + 9728
+# width 32: 32 x (10 mul + 10 add + relu) + 32 x (32 mul + 32 add + relu) + 32 mul + 32 add = 2,816
+REF_OPS_PER_PLACEMENT_WIDE32 = 1010 - 192 + 2816
 METRIC_STRESS = ("beam placements/s on 1 B200 (uneven-length stress: 200 models x 100 games = 20k sims, "
                  "10% v11 champion, cap 10000)")
 METRIC_WIDE = ("beam placements/s on 1 B200 (widened 10-64-64-1 evaluator: 8 islands x 100 models x 100 games "
                "= 80k sims, cap 2000)")
+METRIC_WIDE32 = ("beam placements/s on 1 B200 (widened 10-32-32-1 evaluator: 8 islands x 100 models x 100 games "
+                 "= 80k sims, cap 2000)")
+METRICS = {"wide": METRIC_WIDE, "wide32": METRIC_WIDE32, "stress": METRIC_STRESS}
+HIDDEN = {"wide": 64, "wide32": 32}           # the widened models' hidden width
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
 # on the small-case capture) and its DRAM bytes per full-generation launch
 # (ncu dram__bytes_read.sum + dram__bytes_write.sum, 1-pass capture of the full launch).
@@ -120,19 +126,21 @@ class ClockSampler:
                 if any(r[3].replace('.', '').isdigit() for r in rows) else None}
 
 
-def _ref_lib(wide: bool = False):
+def _ref_lib(hidden: int = 0):
     """The reference's CPU path (oracle/_ref) if built, else the oracle's restatement,
-    as (batch function with the ta3ref_eval_mt signature, kind)."""
+    as (batch function with the ta3ref_eval_mt signature, kind); hidden = 0 for v11,
+    else the widened network's width (64 or 32)."""
     ref = os.path.join(ROOT, "oracle", "_ref", "libta3ref.so")
     if os.path.exists(ref):
         lib = C.CDLL(ref)
-        return (lib.ta3ref_eval_wide_mt if wide else lib.ta3ref_eval_mt), "reference"
+        fn = {0: lib.ta3ref_eval_mt, 64: lib.ta3ref_eval_wide_mt, 32: lib.ta3ref_eval_wide32_mt}[hidden]
+        return fn, "reference"
     port = os.path.join(ROOT, "oracle", "_build", "libta3oracle.so")
     if not os.path.exists(port):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
     lib = C.CDLL(port)
-    if wide:
-        return (lambda *a: lib.ta3o_eval_net_mt(a[0], 64, 64, *a[1:])), "port"
+    if hidden:
+        return (lambda *a: lib.ta3o_eval_net_mt(a[0], hidden, hidden, *a[1:])), "port"
     return lib.ta3o_eval_mt, "port"
 
 
@@ -140,7 +148,7 @@ def cpu_rate(batch: workload.Batch, budget_s: float, threads: int):
     """Placements/s of the CPU path over a bounded sample of the batch: island 0's
     (model, game) pairs in workload order, `threads` games of one model per call
     (one host thread each), until budget_s of work."""
-    f, kind = _ref_lib(batch.weights.shape[1] == workload.NUM_PARAMS_WIDE)
+    f, kind = _ref_lib({workload.NUM_PARAMS_WIDE: 64, workload.NUM_PARAMS_WIDE32: 32}.get(batch.weights.shape[1], 0))
     p = lambda a: a.ctypes.data_as(C.c_void_p)
     games = batch.games
     mpi = batch.models // batch.islands
@@ -176,9 +184,9 @@ def _batch(args, rank: int = 0) -> workload.Batch:
     if args.model == "stress":
         return workload.uneven_batch(models=args.pop or 200, games=args.games or 100, max_moves=args.cap or 10000,
                                      seed=rank_seed(2, rank))
-    if args.model == "wide":
+    if args.model in HIDDEN:
         return workload.wide_batch(islands=args.islands or 8, pop=args.pop or 100, games=args.games or 100,
-                                   max_moves=args.cap or 2000, seed=rank_seed(3, rank))
+                                   max_moves=args.cap or 2000, seed=rank_seed(3, rank), hidden=HIDDEN[args.model])
     return workload.generation_batch(islands=args.islands or 4, pop=args.pop or 50, games=args.games or 50,
                                      max_moves=args.cap or 2000, seed=rank_seed(1, rank))
 
@@ -188,7 +196,7 @@ def run_reference(args):
     if rank != 0:
         return
     batch = _batch(args)
-    metric = {"wide": METRIC_WIDE, "stress": METRIC_STRESS}.get(args.model, METRIC)
+    metric = METRICS.get(args.model, METRIC)
     threads = host_threads()
     rates = []
     kind = "reference"
@@ -233,9 +241,10 @@ def run_ours(args):
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
     # weak scaling: each rank scores its own generation (islands seeded per rank)
     batch = _batch(args, rank)
-    wide = args.model == "wide"
-    metric = {"wide": METRIC_WIDE, "stress": METRIC_STRESS}.get(args.model, METRIC)
-    ops_per_placement = REF_OPS_PER_PLACEMENT_WIDE if wide else REF_OPS_PER_PLACEMENT
+    wide = args.model in HIDDEN
+    metric = METRICS.get(args.model, METRIC)
+    ops_per_placement = {"wide": REF_OPS_PER_PLACEMENT_WIDE, "wide32": REF_OPS_PER_PLACEMENT_WIDE32}.get(
+        args.model, REF_OPS_PER_PLACEMENT)
     ev = ModelEvaluator(device=local)
     stream = torch.cuda.Stream(device=dev)
     w_dev = torch.from_numpy(batch.weights).to(dev)
@@ -364,9 +373,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=-1, help="fixed kernel variant (default: autotune)")
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--model", choices=["v11", "wide", "stress"], default="v11",
-                    help="v11 (headline), the widened 10-64-64-1 evaluator's 80k-sim generation, or the "
-                         "uneven-length stress batch (20k sims, 10%% champion, cap 10000)")
+    ap.add_argument("--model", choices=["v11", "wide", "wide32", "stress"], default="v11",
+                    help="v11 (headline), the widened 10-64-64-1 (wide) or 10-32-32-1 (wide32) evaluator's "
+                         "80k-sim generation, or the uneven-length stress batch (20k sims, 10%% champion, cap 10000)")
     # reduced shapes for profiling captures only (the headline is the default full generation)
     ap.add_argument("--islands", type=int, default=0)
     ap.add_argument("--pop", type=int, default=0)
