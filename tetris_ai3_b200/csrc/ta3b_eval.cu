@@ -566,9 +566,10 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
     uint32_t queued = 0;
     int seg = 0;
     // TA3B_ILP candidates per lane per iteration (c, c+32, ...) in straight-line
-    // code (1 measured fastest on B200: 504 ms per full-generation step vs 694 ms for 2)
     // code, so their dependency chains interleave; out-of-range slots evaluate
-    // the last real candidate and are discarded
+    // the last real candidate and are discarded. 1 measured fastest on B200: 486 ms
+    // per full-generation step vs 681 ms for 2 (no spills at 16 warps per SM) and
+    // 766 ms for 2 at 12 warps per SM.
     for (uint32_t c0 = 0; c0 < total; c0 += TA3B_ILP * WARP) {
         uint32_t info[TA3B_ILP], idx[TA3B_ILP], sg[TA3B_ILP];
         bool valid[TA3B_ILP];
