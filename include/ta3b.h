@@ -160,7 +160,7 @@ int ta3b_select_variant(ta3b_ctx* ctx, int variant);
 
 /* Device self-test of the per-candidate evaluation (tests and tooling): one
  * thread per candidate runs the incremental fast path and the full reference
- * path on caller-built parent records (84 words each, the layout of
+ * path on caller-built parent records (68 words each, the layout of
  * tetris_ai3_b200/csrc/eval_core.h). cand[t] = piece | placement << 8 |
  * held-is-I << 16 | record index << 17. Outputs per candidate: fast status
  * (0 evaluated, 1 deferred) and value, full-path legality and value; dbg32

@@ -2,11 +2,17 @@
 //
 // Same class name, member signatures, argument meaning and error behaviour
 // (std::runtime_error) as the reference's ta3_gpu/incl/ta3/gpu/model_eval.hpp:27-114, so
-// ta3_trainer's TetrisProblem2::evalBatch (ta3_trainer/src/tetris_problem2.cpp:44-72) compiles
-// against it unchanged. eval_host (the CPU parity path) is not provided: the product has no CPU
-// evaluator; parity tooling lives in the repository's oracle/.
+// ta3_trainer's TetrisProblem2::evalBatch (ta3_trainer/src/tetris_problem2.cpp:44-72) and
+// Trainer2::verifyEvaluator (ta3_trainer/src/trainer2.cpp:57-89) compile against it unchanged.
+//
+// eval (the GPU path) calls libta3b.so. eval_host (the CPU parity path) forwards to
+// ta3b_eval_host (ta3b_host_ref.h), which libta3b.so does NOT contain: the caller compiles
+// integration/ta3b_eval_host.cpp into its own binary against the reference's headers, as the
+// reference compiles ta3_gpu/src/common/model_eval_host.cpp. A caller that never calls
+// eval_host needs neither.
 #pragma once
 #include "ta3b.h"
+#include "ta3b_host_ref.h"
 
 #include <cstdint>
 #include <memory>
@@ -42,6 +48,20 @@ public:
     [[nodiscard]] std::vector<float> eval(std::span<weights_t const> weights, std::span<std::uint64_t const> seeds,
                                           std::uint32_t max_moves) {
         return eval(weights, 1u, seeds, max_moves);
+    }
+
+    // model_eval.hpp:62-67: the same games on the CPU, the parity reference for eval; reads the
+    // first NUM_PARAMS weights (one model)
+    [[nodiscard]] static std::vector<float> eval_host(std::span<weights_t const> weights,
+                                                      std::span<std::uint64_t const> seeds, std::uint32_t max_moves) {
+        std::vector<float> out(seeds.size());
+        if (weights.size() < TA3B_NUM_PARAMS)
+            throw std::runtime_error("ta3b: eval_host: weights.size() must be at least NUM_PARAMS");
+        if (ta3b_eval_host(weights.data(), static_cast<std::uint32_t>(weights.size()), seeds.data(),
+                           static_cast<std::uint32_t>(seeds.size()), max_moves, out.data(), nullptr,
+                           nullptr) != TA3B_OK)
+            throw std::runtime_error("ta3b: eval_host: invalid arguments");
+        return out;
     }
 
     // extension: scores plus piece and line counts in one call

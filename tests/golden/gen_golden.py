@@ -170,7 +170,7 @@ def games():
     sw = np.zeros(2 * P, np.float32)
     REF.ta3ref_selfcheck_weights(ptr(sw))                   # trainer2.cpp:57-89
     add("trainer self-check: 2 models, seeds 101/202/303, 100 moves", sw, [101, 202, 303], 100)
-    champ = workload.load_champ("/root/reference/models/v11_16_32_32_score_296.champ")
+    champ = workload.champion()        # the reference's models/v11_16_32_32_score_296.champ, byte for byte
     add("v11 champion, seeds 0..29, cap 300", champ, list(range(30)), 300)
     add("v11 champion, seed 0, cap 2000", champ, [0], 2000)
     rng = np.random.default_rng(7)

@@ -86,13 +86,14 @@ def build_oracle() -> None:
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
 
 
-def build_reference_cpu() -> bool:
-    """Compile the reference's own CPU path into oracle/_ref (only where the
-    reference checkout exists; elsewhere the prebuilt library is used)."""
-    ref = os.environ.get("TA3_REFERENCE", "/root/reference")
-    if not os.path.isdir(os.path.join(ref, "ta3_sim")):
+def build_reference_cpu(ref: str | None = None) -> bool:
+    """Compile the reference's own CPU path into oracle/_ref from the checkout
+    at `ref` (default: the TA3_REFERENCE environment variable). Without a
+    checkout nothing is built and the prebuilt library, if any, is used."""
+    ref = ref or os.environ.get("TA3_REFERENCE")
+    if not ref or not os.path.isdir(os.path.join(ref, "ta3_sim")):
         return False
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={ref}"], check=True)
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), f"REF={ref}", "ref"], check=True)
     return True
 
 
