@@ -104,8 +104,10 @@ int ta3b_eval_islands(ta3b_ctx* ctx, const float* weights, uint32_t num_islands,
  * the call first repacks the weights into the kernel's layout (16-byte aligned,
  * layers 1 and 2 transposed, a per-model flag) in a copy owned by the context;
  * that copy is allocated by the first widened call of a larger size, so make
- * such a call once before capturing it. No reference counterpart (the
- * reference stages host buffers). */
+ * such a call once before capturing it. The call returns before the kernel
+ * runs, so a device-side error is read afterwards with ta3b_device_status.
+ * At most 2^32 - 1 sims per call (as for every context entry point). No
+ * reference counterpart (the reference stages host buffers). */
 int ta3b_eval_device(ta3b_ctx* ctx, const float* d_weights, uint32_t num_islands, uint32_t models_per_island,
                      uint32_t num_params, const uint64_t* d_seeds, uint32_t num_games, uint32_t max_moves,
                      float* d_score, uint32_t* d_pieces, uint32_t* d_lines, uint32_t* d_evals, void* stream);
@@ -115,20 +117,43 @@ int ta3b_eval_device(ta3b_ctx* ctx, const float* d_weights, uint32_t num_islands
  * all device memory; a scheduler thread that cannot afford cudaMalloc's implicit
  * device synchronisation). No context: pass device inputs and outputs and a
  * stream (NULL = legacy default stream); nothing is allocated. The kernel's only
- * scratch -- its work-queue ticket and error status -- is a 256-byte static
- * device array that every GPU loading this library keeps until exit. The first
+ * scratch -- its 64-bit work-queue ticket and error status word -- is a
+ * 256-byte static device array that every GPU loading this library keeps
+ * until exit. The first
  * call on each device sets that device up (resolves the array's address,
  * configures the kernel) with the device current; make that first call before
  * any stream capture. Every call shares the one array and clears it on entry,
  * so calls whose kernels overlap on the GPU race: run them on one stream or
- * serialise them. A call may cover at most 2^32 - 65 sims; larger batches,
+ * serialise them. A call may cover at most 2^32 - 1 sims; larger batches,
  * num_params != 97 and null pointers are rejected with TA3B_ERR_ARG and, when
  * error_out is not NULL, a static message in *error_out. Enqueued, not
- * synchronised. No counterpart in the reference. */
+ * synchronised; ta3b_noalloc_status reads the kernel's status word afterwards.
+ * No counterpart in the reference. */
 int ta3b_eval_device_noalloc(const float* d_weights, uint32_t num_islands, uint32_t models_per_island,
                              uint32_t num_params, const uint64_t* d_seeds, uint32_t num_games, uint32_t max_moves,
                              float* d_score, uint32_t* d_pieces, uint32_t* d_lines, uint32_t* d_evals,
                              void* stream, const char** error_out);
+
+/* The status word of the most recent ta3b_eval_device_noalloc call on the
+ * current device (0 = no error; any set bit is a device error, bit 0 = a
+ * search found no move although a root placement was legal), copied on
+ * `stream` (NULL = legacy default stream) after the work already queued there,
+ * then that stream is synchronised. Allocates nothing. Returns TA3B_OK for
+ * status 0, TA3B_ERR_DEVICE otherwise, TA3B_ERR_ARG before the first
+ * allocation-free call on the device. Like the evaluation it shares the static
+ * array with every call, so read it before the next call's kernel starts. No
+ * counterpart in the reference. */
+int ta3b_noalloc_status(void* stream, uint32_t* status_out, const char** error_out);
+
+/* Status word of the context's most recent launch (any entry point; after
+ * ta3b_eval_device, once the stream it ran on has finished): 0 = no error,
+ * bit 1 = the time budget ran out, any other bit = a device error (bit 0: a
+ * search found no move although a root placement was legal). Synchronises the
+ * context's stream. Returns TA3B_OK, TA3B_ERR_TIMEOUT or TA3B_ERR_DEVICE
+ * accordingly; status_out may be NULL. The host-buffer entry points check this
+ * word themselves. No reference counterpart (the reference's kernel reports
+ * no device status). */
+int ta3b_device_status(ta3b_ctx* ctx, uint32_t* status_out);
 
 /* Per-move trace of every sim (debug / parity tooling): trace_out receives
  * 3 bytes per move (hold, orientation, x + 2), max_moves moves per sim,

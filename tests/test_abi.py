@@ -159,3 +159,22 @@ def test_surrogate_header_is_exported():
     assert names == SURROGATE_EXPORTS
     lib = library()
     assert [n for n in names if not hasattr(lib, n)] == []
+
+
+def test_noalloc_sim_bound_is_checked_before_any_device_call(lib):
+    """The work queue's ticket is 64-bit and sim indices are 32-bit: a call may cover up to
+    2^32 - 1 sims. The bound is checked on the host before anything touches a device."""
+    err = C.c_char_p()
+    # 65536 x 65536 x 1 = 2^32 sims: one too many
+    rc = lib.ta3b_eval_device_noalloc(None, 65536, 65536, 97, None, 1, 10, None, None, None, None, None,
+                                      C.byref(err))
+    assert rc == -1 and b"too many sims" in err.value and b"2^32 - 1" in err.value
+    # 65535 x 65537 x 1 = 2^32 - 1 sims: within the bound, so the next check (null pointers) answers
+    rc = lib.ta3b_eval_device_noalloc(None, 65535, 65537, 97, None, 1, 10, None, None, None, None, None,
+                                      C.byref(err))
+    assert rc == -1 and b"null" in err.value
+    assert lib.ta3b_noalloc_status(None, None, C.byref(err)) == -1 and b"null" in err.value
+
+
+def test_status_query_rejects_a_null_context(lib):
+    assert lib.ta3b_device_status(None, None) == -1

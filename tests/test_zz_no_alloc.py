@@ -48,9 +48,13 @@ def test_noalloc_matches_context_path_twice():
                                           ptr(out[0]), ptr(out[1]), ptr(out[2]), ptr(out[3]),
                                           C.c_void_p(stream.cuda_stream), C.byref(err))
         assert rc == 0, err.value
+        status = C.c_uint32(0xFFFFFFFF)
+        assert lib.ta3b_noalloc_status(C.c_void_p(stream.cuda_stream), C.byref(status), C.byref(err)) == 0, err.value
+        assert status.value == 0
         torch.cuda.synchronize()
         for a, r in zip(out, ref):
             assert torch.equal(a.view(torch.int32), r.view(torch.int32)), f"call {call}"
+    assert ev.device_status() == 0
     ev.close()
 
 
@@ -64,7 +68,7 @@ def test_noalloc_rejects_oversized_and_bad_arguments():
     o = torch.zeros(1, dtype=torch.float32, device="cuda")
     ptr = lambda t: C.c_void_p(t.data_ptr())
     err = C.c_char_p()
-    # 2^32 sims: beyond the 32-bit work queue the static scratch holds
+    # 2^32 sims: one more than a call may cover (sim indices are 32-bit)
     rc = lib.ta3b_eval_device_noalloc(ptr(w), 65536, 65536, 97, ptr(s), 1, 10, ptr(o), None, None, None, None,
                                       C.byref(err))
     assert rc != 0 and b"too many sims" in err.value

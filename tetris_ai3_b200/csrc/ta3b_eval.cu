@@ -35,6 +35,12 @@ namespace {
 
 constexpr int WARP = 32;
 constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
+// The work queue's scratch words: a 64-bit sim ticket (words 0-1) and the error status (word 2:
+// bit 0 = a search found no move although a root was legal, bit 1 = the time budget ran out).
+constexpr int kStatusWord = 2;
+constexpr size_t kScratchBytes = 16;
+constexpr uint32_t kNoSim = 0xFFFFFFFFu;                 // never a sim index: sims <= 2^32 - 1
+constexpr uint64_t kMaxSims = 0xFFFFFFFFull;
 
 // ---------------------------------------------------------------- tables ---
 struct DevTables {
@@ -447,7 +453,7 @@ struct Params {
     uint8_t* trace;
     uint32_t* n_moves;
     uint32_t* board_out;
-    uint32_t* scratch;                 // [0] sim ticket, [1] error status
+    uint32_t* scratch;                 // 16-byte aligned: [0..1] 64-bit sim ticket, [2] error status
     unsigned long long* timing;        // optional: per sim [start, end] global timer (ns)
     unsigned long long budget_ns;      // 0, or the launch's time budget: past it warps stop and set status bit 2
     uint32_t num_games, models_per_island, max_moves, total_sims;
@@ -824,10 +830,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     // kept in shared memory so it costs no register in the move loop
     if (BUDGET && lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ws.t_start));
     for (;;) {
+        // a 64-bit ticket: every resident warp draws one past the last sim, which a 32-bit
+        // counter could wrap near 2^32 sims; kNoSim (no sim index is that large) ends the warp
         uint32_t sim = 0;
-        if (lane == 0) sim = atomicAdd(&p.scratch[0], 1u);
+        if (lane == 0) {
+            unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
+            sim = t < p.total_sims ? uint32_t(t) : kNoSim;
+        }
         sim = __shfl_sync(FULL_MASK, sim, 0);
-        if (sim >= p.total_sims) break;
+        if (sim == kNoSim) break;
         uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
@@ -850,7 +861,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         __syncwarp();
         uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move<NET>(ws, lut, fw, hb, lane, evals, &p.scratch[1]);
+            Move const mv = search_move<NET>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
             if (mv.none) break;
             if (lane == 0) {
                 if (p.trace) {
@@ -872,7 +883,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                     unsigned long long now;
                     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
                     if (now - ws.t_start > p.budget_ns) {
-                        atomicOr(&p.scratch[1], 2u);
+                        atomicOr(&p.scratch[kStatusWord], 2u);
                         ws.eng.over = 3;
                     }
                 }
@@ -1076,7 +1087,7 @@ int check_sizes(ta3b_ctx* ctx, uint32_t num_islands, uint32_t models_per_island,
                                            std::to_string(NPARAMS_WIDE) + " (10 -> 64 -> 64 -> 1) or " +
                                            std::to_string(NPARAMS_WIDE32) + " (10 -> 32 -> 32 -> 1)");
     uint64_t const sims = uint64_t(num_islands) * models_per_island * num_games;
-    if (sims > 0xFFFFFFF0ull) return fail(ctx, TA3B_ERR_ARG, "too many sims in one batch");
+    if (sims > kMaxSims) return fail(ctx, TA3B_ERR_ARG, "too many sims in one batch (at most 2^32 - 1)");
     return TA3B_OK;
 }
 
@@ -1129,7 +1140,7 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     bool const budget = ctx->budget_ns != 0;
     if (budget && !ctx->budget_grid[ni])
         if (int rc = setup_kernel(ctx, kBudgetNet[ni], ni, ctx->budget_grid[ni], "budget kernel")) return rc;
-    TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, 2 * sizeof(uint32_t), st), "reset work queue");
+    TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, kScratchBytes, st), "reset work queue");
     // with a time budget the budget-checking flavour runs (its own fixed launch shape)
     Variant const* const v = budget ? &kBudgetNet[ni] : ni != NET_V11 ? &kWideNet[ni] : &kVariants[ctx->variant];
     uint32_t const warps = v->warps;
@@ -1145,12 +1156,19 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     return TA3B_OK;
 }
 
+int status_code(ta3b_ctx* ctx, uint32_t status);
+
 int read_status(ta3b_ctx* ctx) {
     uint32_t status = 0;
-    TA3B_CUDA(ctx, cudaMemcpyAsync(&status, ctx->d_scratch + 1, sizeof status, cudaMemcpyDeviceToHost, ctx->stream),
-              "read status");
+    TA3B_CUDA(ctx, cudaMemcpyAsync(&status, ctx->d_scratch + kStatusWord, sizeof status, cudaMemcpyDeviceToHost,
+                                   ctx->stream), "read status");
     TA3B_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "kernel run");
-    if (status & 1u) return fail(ctx, TA3B_ERR_DEVICE, "kernel reported status " + std::to_string(status));
+    return status_code(ctx, status);
+}
+
+// the call's result for a status word: bit 1 = the time budget ran out, any other bit = a device error
+int status_code(ta3b_ctx* ctx, uint32_t status) {
+    if (status & ~2u) return fail(ctx, TA3B_ERR_DEVICE, "kernel reported status " + std::to_string(status));
     if (status & 2u)
         return fail(ctx, TA3B_ERR_TIMEOUT, "time budget exceeded: the launch stopped early, results are incomplete");
     return TA3B_OK;
@@ -1297,7 +1315,8 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
     ctx->sms = uint32_t(prop.multiProcessorCount);
     if (cudaSetDevice(c.device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&ctx->d_scratch, 4 * sizeof(uint32_t)) != cudaSuccess) {
+        cudaMalloc(&ctx->d_scratch, kScratchBytes) != cudaSuccess ||
+        cudaMemset(ctx->d_scratch, 0, kScratchBytes) != cudaSuccess) {
         g_create_error = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());
         ta3b_destroy(ctx);
         return nullptr;
@@ -1480,6 +1499,17 @@ int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_bl
     return TA3B_OK;
 }
 
+int ta3b_device_status(ta3b_ctx* ctx, uint32_t* status_out) {
+    if (!ctx) return TA3B_ERR_ARG;
+    TA3B_CUDA(ctx, cudaSetDevice(ctx->device), "set device");
+    uint32_t status = 0;
+    TA3B_CUDA(ctx, cudaMemcpyAsync(&status, ctx->d_scratch + kStatusWord, sizeof status, cudaMemcpyDeviceToHost,
+                                   ctx->stream), "read status");
+    TA3B_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "read status");
+    if (status_out) *status_out = status;
+    return status_code(ctx, status);
+}
+
 } // extern "C"
 
 // ============================================ allocation-free evaluation ===
@@ -1489,14 +1519,16 @@ int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_bl
 // critical scheduler thread that must not pay cudaMalloc/cudaFree's implicit
 // device-wide synchronisation. ta3b_eval_device_noalloc serves them: it creates
 // no context and allocates nothing. The caller passes device inputs and
-// outputs; the only scratch the evaluation kernel needs -- its work-queue
-// ticket and error status word -- lives in the file-scope array below, which
-// every GPU that loads this library holds until the process exits.
+// outputs; the only scratch the evaluation kernel needs -- its 64-bit work-queue
+// ticket (words 0-1) and error status word (word 2) -- lives in the file-scope
+// array below, which every GPU that loads this library holds until the process
+// exits.
 namespace {
 
-constexpr uint32_t kNoAllocScratchWords = 64;                 // 256 bytes; words 0 (ticket) and 1 (status) used
-constexpr uint64_t kNoAllocMaxSims = 0xFFFFFFFFull - 64u;     // the 32-bit ticket must not wrap
+constexpr uint32_t kNoAllocScratchWords = 64;                 // 256 bytes; words 0-2 used
+constexpr uint64_t kNoAllocMaxSims = kMaxSims;                // the 64-bit ticket cannot wrap
 static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocScratchWords];
+static_assert(kScratchBytes <= sizeof(g_noalloc_scratch), "the work-queue words fit the static array");
 
 constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocDevice {
@@ -1521,7 +1553,7 @@ extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_isl
     if (num_params != NPARAMS) return fail_static(TA3B_ERR_ARG, "num_params must be 97 (v11 value model)");
     uint64_t const sims = uint64_t(num_islands) * models_per_island * num_games;
     if (sims > kNoAllocMaxSims)
-        return fail_static(TA3B_ERR_ARG, "too many sims for the allocation-free path (at most 2^32 - 65 per call)");
+        return fail_static(TA3B_ERR_ARG, "too many sims for the allocation-free path (at most 2^32 - 1 per call)");
     if (sims == 0) return TA3B_OK;
     if (!d_weights || !d_seeds || !d_score) return fail_static(TA3B_ERR_ARG, "null device pointer");
     int dev = 0;
@@ -1554,7 +1586,7 @@ extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_isl
     NoAllocDevice const& d = g_noalloc_dev[dev];
     cudaStream_t const st = static_cast<cudaStream_t>(stream);
     // the array keeps the previous call's contents: the ticket and status must start at zero
-    if (cudaMemsetAsync(d.scratch, 0, 2 * sizeof(uint32_t), st) != cudaSuccess)
+    if (cudaMemsetAsync(d.scratch, 0, kScratchBytes, st) != cudaSuccess)
         return fail_static(TA3B_ERR_CUDA, "clearing the scratch array failed");
     Params prm{};
     prm.weights = d_weights;
@@ -1571,5 +1603,43 @@ extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_isl
     uint32_t const need = uint32_t((sims + var.warps - 1) / var.warps);
     var.fn<<<need < d.grid ? need : d.grid, var.warps * 32, dyn, st>>>(prm);
     if (cudaGetLastError() != cudaSuccess) return fail_static(TA3B_ERR_CUDA, "kernel launch failed");
+    return TA3B_OK;
+}
+
+// The status word the most recent allocation-free call on the current device left
+// in the static array: copied on `stream` (NULL = legacy default stream) after the
+// work already queued there, which must include that call. Allocates nothing.
+extern "C" int ta3b_noalloc_status(void* stream, uint32_t* status_out, char const** error_out) {
+    if (error_out) *error_out = "";
+    if (!status_out) {
+        if (error_out) *error_out = "null status_out";
+        return TA3B_ERR_ARG;
+    }
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices) {
+        if (error_out) *error_out = "cudaGetDevice failed or device ordinal too large";
+        return TA3B_ERR_CUDA;
+    }
+    uint32_t* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mu);
+        if (g_noalloc_dev[dev].ready) scratch = g_noalloc_dev[dev].scratch;
+    }
+    if (!scratch) {
+        if (error_out) *error_out = "no allocation-free evaluation has run on this device";
+        return TA3B_ERR_ARG;
+    }
+    cudaStream_t const st = static_cast<cudaStream_t>(stream);
+    uint32_t status = 0;
+    if (cudaMemcpyAsync(&status, scratch + kStatusWord, sizeof status, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess) {
+        if (error_out) *error_out = "reading the status word failed";
+        return TA3B_ERR_CUDA;
+    }
+    *status_out = status;
+    if (status) {
+        if (error_out) *error_out = "the kernel reported a device error status";
+        return TA3B_ERR_DEVICE;
+    }
     return TA3B_OK;
 }

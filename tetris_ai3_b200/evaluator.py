@@ -32,7 +32,8 @@ _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
            "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
-           "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc", "ta3b_set_time_budget"]
+           "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc", "ta3b_set_time_budget",
+           "ta3b_device_status", "ta3b_noalloc_status"]
 
 
 class EvaluatorError(RuntimeError):
@@ -72,6 +73,8 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
     lib.ta3b_eval_device_noalloc.argtypes = [vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp,
                                              C.POINTER(C.c_char_p)]
+    lib.ta3b_noalloc_status.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_char_p)]
+    lib.ta3b_device_status.argtypes = [vp, C.POINTER(C.c_uint32)]
     if path is None:
         _lib = lib
     return lib
@@ -199,6 +202,13 @@ class ModelEvaluator:
         self._check(self._lib.ta3b_eval_device(self._ctx, ptr(weights), islands, models // islands, nparams,
                                                ptr(seeds), games, max_moves, ptr(score), ptr(pieces), ptr(lines),
                                                ptr(evals), st))
+
+    def device_status(self) -> int:
+        """Status word of the context's most recent launch (0 = no error); raises on a non-zero
+        status. After eval_device, call it once the stream the batch ran on has finished."""
+        st = C.c_uint32()
+        self._check(self._lib.ta3b_device_status(self._ctx, C.byref(st)))
+        return st.value
 
     def set_time_budget(self, seconds: float):
         """Per-launch time budget (0 = none): past it the call raises with an incomplete batch."""
