@@ -158,11 +158,17 @@ int ta3b_device_status(ta3b_ctx* ctx, uint32_t* status_out);
 /* Per-move trace of every sim (debug / parity tooling): trace_out receives
  * 3 bytes per move (hold, orientation, x + 2), max_moves moves per sim,
  * model-major; n_moves_out the number of searched moves per sim;
- * board_out the final 10 bit-columns per sim. Host buffers. */
+ * board_out the final 10 bit-columns per sim. keys_out (may be NULL; 2 x
+ * max_moves per sim) receives, per searched move, the two largest keys of the
+ * final argmax (leaf keys and dead-end fallbacks; ta3_ai/incl/ta3/ai/search/
+ * beam.hpp:204-224,407-443): (ordered value bits << 32) | (2192 - order), so
+ * key1 decodes to the chosen move's value and key1 - key2's values is the
+ * decision's top-two margin. With keys_out the launch runs a tracing flavour
+ * of the kernel, which ignores the time budget. Host buffers. */
 int ta3b_eval_trace(ta3b_ctx* ctx, const float* weights, uint32_t num_models, uint32_t num_params,
                     const uint64_t* seeds, uint32_t num_games, uint32_t max_moves,
                     float* score_out, uint32_t* pieces_out, uint32_t* lines_out, uint32_t* evals_out,
-                    uint8_t* trace_out, uint32_t* n_moves_out, uint32_t* board_out);
+                    uint8_t* trace_out, uint32_t* n_moves_out, uint32_t* board_out, uint64_t* keys_out);
 
 /* Scheduling profile of one island-batched evaluation (tooling): like
  * ta3b_eval_islands plus, per sim, the number of evaluated placements and the

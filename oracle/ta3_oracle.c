@@ -466,7 +466,9 @@ typedef struct { int orient, x, hold; float value; int none; } result_t;
 static uint32_t clear_bump(int cleared) { return cleared == 0 ? 0u : 1u << (8 * (cleared - 1)); }  /* model_defs.hpp:37-43 */
 
 /* beam.hpp:484-570 (search_move_beam) with the stages of beam.hpp:283-470 */
-static result_t search_move_beam(engine_t const* g, net_t const* w, uint64_t* evals) {
+/* top2 (may be NULL) receives the best and the second-best key of the final argmax
+ * (leaf keys and the dead-end fallbacks alike): diagnostics for divergence triage */
+static result_t search_move_beam(engine_t const* g, net_t const* w, uint64_t* evals, uint64_t* top2) {
     result_t res = {0, 0, 0, -INFINITY, 1};
     if (g->over) return res;
     enum { ROOT_SLOTS = 2 * MP, MID_SLOTS = 32 * 2 * MP, LEAF_ORDERS = 32 * 2 * MP, SPAN = LEAF_ORDERS + 16 };
@@ -497,8 +499,9 @@ static result_t search_move_beam(engine_t const* g, net_t const* w, uint64_t* ev
     uint32_t const root_count = select_top(root_scores, ROOT_SLOTS, KS[0], top_root_slot, top_root_score);
     if (root_count == 0) return res;
 
-    uint64_t best_key = 0;
-#define CONSIDER(sc, ord) do { uint64_t const k_ = ((uint64_t)(sc) << 32) | (uint64_t)(SPAN - (ord)); if (k_ > best_key) best_key = k_; } while (0)
+    uint64_t best_key = 0, second_key = 0;
+#define CONSIDER(sc, ord) do { uint64_t const k_ = ((uint64_t)(sc) << 32) | (uint64_t)(SPAN - (ord)); \
+    if (k_ > best_key) { second_key = best_key; best_key = k_; } else if (k_ > second_key) second_key = k_; } while (0)
 
     frontier_t kept[2];
     uint32_t cur = 0, kept_count = root_count;
@@ -587,6 +590,7 @@ static result_t search_move_beam(engine_t const* g, net_t const* w, uint64_t* ev
     res.orient = pl0.orient; res.x = pl0.x; res.hold = rn->root_hold;
     res.value = ordered_bits_inv((uint32_t)(best_key >> 32));
     res.none = res.value == -INFINITY;                     /* search.hpp:41 */
+    if (top2) { top2[0] = best_key; top2[1] = second_key; }
     return res;
 }
 
@@ -621,13 +625,14 @@ static double score_v1(stats_t const* s) {                /* score_v1.hpp:8-34 *
 /* ------------------------------------------------------- C ABI ------ */
 /* model_eval_host.cpp:35-51: one game, optional per-move trace (hold, orientation, x+2) */
 static int play_net(net_t const* w, uint64_t seed, uint32_t max_moves, float* score, uint32_t* pieces,
-                    uint32_t* lines, uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint32_t* board_out) {
+                    uint32_t* lines, uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint32_t* board_out,
+                    uint64_t* keys) {
     ensure_ready();
     engine_t g; engine_reset(&g, seed);
     stats_t st; memset(&st, 0, sizeof st);
     uint64_t ev = 0; uint32_t moves = 0;
     for (uint32_t i = 0; i < max_moves && !g.over; ++i) {
-        result_t const r = search_move_beam(&g, w, &ev);
+        result_t const r = search_move_beam(&g, w, &ev, keys ? keys + 2 * moves : NULL);
         if (r.none) break;
         if (trace) { trace[3 * moves] = (uint8_t)r.hold; trace[3 * moves + 1] = (uint8_t)r.orient; trace[3 * moves + 2] = (uint8_t)(r.x + 2); }
         ++moves;
@@ -647,7 +652,15 @@ static int play_net(net_t const* w, uint64_t seed, uint32_t max_moves, float* sc
 int ta3o_play(float const* w, uint64_t seed, uint32_t max_moves, float* score, uint32_t* pieces, uint32_t* lines,
               uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint32_t* board_out) {
     net_t const net = {w, NHID, 0};
-    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, board_out);
+    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, board_out, NULL);
+}
+
+/* ta3o_play plus, per searched move, the best and second-best key of the final argmax
+ * (keys: 2 x max_moves; (ordered value bits << 32) | (span - order)) */
+int ta3o_play_keys(float const* w, uint64_t seed, uint32_t max_moves, float* score, uint32_t* pieces,
+                   uint32_t* lines, uint64_t* evals, uint8_t* trace, uint32_t* n_moves, uint64_t* keys) {
+    net_t const net = {w, NHID, 0};
+    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, NULL, keys);
 }
 
 /* one game of a dense value network with hidden widths h1, h2 (h2 = 0: one hidden layer) */
@@ -656,7 +669,7 @@ int ta3o_play_net(float const* w, uint32_t h1, uint32_t h2, uint64_t seed, uint3
                   uint32_t* board_out) {
     if (h1 == 0 || h1 > MAXH || h2 > MAXH) return 1;
     net_t const net = {w, h1, h2};
-    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, board_out);
+    return play_net(&net, seed, max_moves, score, pieces, lines, evals, trace, n_moves, board_out, NULL);
 }
 
 uint32_t ta3o_net_params(uint32_t h1, uint32_t h2) { return net_params(h1, h2); }
@@ -696,7 +709,7 @@ static void* mt_worker(void* arg) {
         if (i >= total) break;
         uint64_t e = 0; float s; uint32_t p, l;
         net_t const net = {j->w + (i / j->num_games) * net_params(j->h1, j->h2), j->h1, j->h2};
-        play_net(&net, j->seeds[i % j->num_games], j->max_moves, &s, &p, &l, &e, 0, 0, 0);
+        play_net(&net, j->seeds[i % j->num_games], j->max_moves, &s, &p, &l, &e, 0, 0, 0, 0);
         j->score[i] = s;
         if (j->pieces) j->pieces[i] = p;
         if (j->lines) j->lines[i] = l;
@@ -774,7 +787,7 @@ void ta3o_piece_sequence(uint64_t seed, uint32_t n, uint8_t* out) {
     for (uint32_t i = 0; i < n; ++i) { out[i] = g.queue[0]; advance_queue(&g); }
 }
 
-void ta3o_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* out) {   /* model_eval.hpp:148-151 */
+void ta3o_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* out) {   /* model_eval.hpp:84-103 */
     rng_t r; rng_seed(&r, seed);
     for (uint32_t i = 0; i < games; ++i) out[i] = rng_next(&r);
 }

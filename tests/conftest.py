@@ -84,3 +84,31 @@ def host():
         b.build_host()
     from tetris_ai3_b200 import trainer
     return trainer
+
+
+def oracle_play_keys(lib, w: np.ndarray, seed: int, max_moves: int):
+    """One game on the oracle with per-move top-two final keys: (trace bytes, n_moves, keys (n, 2))."""
+    w = np.ascontiguousarray(w, dtype=np.float32).reshape(97)
+    s, p, l, e, nm = C.c_float(), C.c_uint32(), C.c_uint32(), C.c_uint64(), C.c_uint32()
+    tr = np.zeros(3 * max(max_moves, 1), np.uint8)
+    keys = np.zeros((max(max_moves, 1), 2), np.uint64)
+    lib.ta3o_play_keys(ptr(w), C.c_uint64(int(seed)), max_moves, C.byref(s), C.byref(p), C.byref(l), C.byref(e),
+                       ptr(tr), C.byref(nm), ptr(keys))
+    return tr[:3 * nm.value].tobytes(), nm.value, keys[:nm.value]
+
+
+def first_divergence(trace_a: bytes, trace_b: bytes, keys_a, keys_b):
+    """The first move where two traces differ, with each side's top-two margin there, or None.
+    A divergence between two bit-exact paths can only come from a value that rounds differently;
+    the margin says how close that decision was."""
+    from tetris_ai3_b200.evaluator import decode_key, top2_margin
+    n = min(len(trace_a), len(trace_b)) // 3
+    for m in range(n):
+        if trace_a[3 * m:3 * m + 3] != trace_b[3 * m:3 * m + 3]:
+            side = lambda k: {"best": decode_key(k[m][0]), "second": decode_key(k[m][1]),
+                              "margin": top2_margin(k[m][0], k[m][1])}
+            return {"move": m, "a": trace_a[3 * m:3 * m + 3].hex(), "b": trace_b[3 * m:3 * m + 3].hex(),
+                    "keys_a": side(keys_a), "keys_b": side(keys_b)}
+    if len(trace_a) != len(trace_b):
+        return {"move": n, "a": trace_a[3 * n:3 * n + 3].hex(), "b": trace_b[3 * n:3 * n + 3].hex()}
+    return None

@@ -4,10 +4,12 @@ inputs, and size-independent properties at full configuration sizes.
 Bit-exact throughout: scores compare as float32 bit patterns."""
 from __future__ import annotations
 
+from concurrent.futures import ThreadPoolExecutor
+
 import numpy as np
 import pytest
 
-from conftest import f32_from_hex, oracle_eval, weights_from_hex
+from conftest import f32_from_hex, first_divergence, oracle_eval, oracle_play_keys, weights_from_hex
 
 pytestmark = pytest.mark.gpu
 
@@ -20,7 +22,15 @@ def ev():
     e.close()
 
 
-def _check_golden_case(ev, case):
+def _divergence(ev, oracle, w, seed, max_moves):
+    """The first move where the device and the oracle part, with both sides' top-two margins."""
+    out = ev.eval_trace(w, 1, np.array([seed], np.uint64), max_moves, keys=True)
+    nm = int(out["moves"][0])
+    otr, _, okeys = oracle_play_keys(oracle, w, seed, max_moves)
+    return first_divergence(bytes(out["trace"][0][:3 * nm]), otr, out["keys"][0][:nm], okeys)
+
+
+def _check_golden_case(ev, case, oracle=None):
     w = weights_from_hex(case["weights"])
     seeds = np.array([int(s) for s in case["seeds"]], np.uint64)
     out = ev.eval_trace(w, w.shape[0], seeds, case["max_moves"])
@@ -28,6 +38,9 @@ def _check_golden_case(ev, case):
     for i, r in enumerate(flat):
         where = f'{case["name"]} sim {i}'
         nm = int(out["moves"][i])
+        if oracle is not None and bytes(out["trace"][i][:3 * nm]).hex() != r["trace"]:
+            m, g = divmod(i, seeds.size)
+            where += f" divergence {_divergence(ev, oracle, w.reshape(-1, 97)[m], int(seeds[g]), case['max_moves'])}"
         assert bytes(out["trace"][i][:3 * nm]).hex() == r["trace"], where
         assert out["score"][i].tobytes() == f32_from_hex(r["score"]).tobytes(), where
         assert (int(out["pieces"][i]), int(out["lines"][i]), int(out["evals"][i]), nm) == \
@@ -35,9 +48,35 @@ def _check_golden_case(ev, case):
         assert out["board"][i].tolist() == r["board"], where
 
 
-def test_golden_games_bit_exact(ev, golden_games):
+def test_golden_games_bit_exact(ev, golden_games, oracle):
     for case in golden_games["cases"]:
-        _check_golden_case(ev, case)
+        _check_golden_case(ev, case, oracle)
+
+
+def test_trace_keys_match_oracle(ev, oracle, golden_games):
+    """Per move, the device's two largest final keys (the tracing flavour) equal the oracle's bit
+    for bit, so every decision's top-two margin is the reference algorithm's; the tracing flavour
+    plays the same games as the ordinary kernel."""
+    from tetris_ai3_b200 import workload
+    from tetris_ai3_b200.evaluator import top2_margin
+    case = next(c for c in golden_games["cases"] if c["name"].startswith("parity_test multi-model"))
+    w = np.concatenate([weights_from_hex(case["weights"]).reshape(-1, 97),
+                        np.stack([(s * workload.normal(8100 + k, 97)).astype(np.float32)
+                                  for k, s in enumerate([0.3, 1.0, 2.0])])])
+    seeds = np.array([int(s) for s in case["seeds"]], np.uint64)
+    out = ev.eval_trace(w, w.shape[0], seeds, 200, keys=True)
+    plain = ev.eval_trace(w, w.shape[0], seeds, 200)
+    assert plain["trace"].tobytes() == out["trace"].tobytes() and plain["score"].tobytes() == out["score"].tobytes()
+    margins = []
+    for i in range(w.shape[0] * seeds.size):
+        m, g = divmod(i, seeds.size)
+        nm = int(out["moves"][i])
+        otr, onm, okeys = oracle_play_keys(oracle, w[m], int(seeds[g]), 200)
+        rep = first_divergence(bytes(out["trace"][i][:3 * nm]), otr, out["keys"][i][:nm], okeys)
+        assert rep is None and nm == onm, f"sim {i}: {rep}"
+        assert np.array_equal(out["keys"][i][:nm], okeys), f"sim {i}"
+        margins += [top2_margin(a, b) for a, b in okeys if b]
+    assert min(margins) >= 0.0
 
 
 def test_single_model_matches_golden(ev, golden_games):
@@ -125,12 +164,20 @@ def test_full_generation_properties(ev, oracle):
     sc2, pc2, lc2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
     assert sc1.tobytes() == sc2.tobytes() and np.array_equal(pc1, pc2)
     assert (pc1 <= b.max_moves).all() and (lc1 <= 4 * pc1).all()
-    # sample: the shortest 24 sims of island 0 replayed by the oracle
-    idx = np.argsort(pc1[:50 * 50], kind="stable")[:24]
-    for i in idx:
+    # samples of island 0 replayed by the oracle: the 24 shortest sims (early deaths) and the 16
+    # longest (cap-reaching CMA candidates, which carry most of the placements), one host thread each
+    order = np.argsort(pc1[:50 * 50], kind="stable")
+    idx = np.concatenate([order[:24], order[-16:]])
+    assert pc1[order[-16:]].min() >= 1000, "the longest sims of the generation play long games"
+
+    def replay(i):
         m, g = divmod(int(i), 50)
         osc, opc, olc, _ = oracle_eval(oracle, b.weights[m], b.seeds[0][g:g + 1], b.max_moves, threads=1)
-        assert osc[0].tobytes() == sc1[i].tobytes() and opc[0] == pc1[i] and olc[0] == lc1[i]
+        return int(i), osc[0], int(opc[0]), int(olc[0])
+
+    with ThreadPoolExecutor(max_workers=16) as pool:
+        for i, osc, opc, olc in pool.map(replay, idx):
+            assert (osc.tobytes(), opc, olc) == (sc1[i].tobytes(), int(pc1[i]), int(lc1[i])), f"sim {i}"
 
 
 def test_device_core_matches_host_core(ev):

@@ -455,6 +455,7 @@ struct Params {
     uint32_t* board_out;
     uint32_t* scratch;                 // 16-byte aligned: [0..1] 64-bit sim ticket, [2] error status
     unsigned long long* timing;        // optional: per sim [start, end] global timer (ns)
+    unsigned long long* keys;          // tracing flavour: per move the final argmax's two largest keys
     unsigned long long budget_ns;      // 0, or the launch's time budget: past it warps stop and set status bit 2
     uint32_t num_games, models_per_island, max_moves, total_sims;
 };
@@ -462,14 +463,38 @@ struct Params {
 struct Move {
     int orient, x, hold;
     bool none;
+    uint64_t key1, key2;               // tracing flavour: the final argmax's two largest keys
 };
 
 struct LevelAcc {
     uint64_t thr;                      // list[k-1], the key a candidate must beat
     uint64_t list;                     // top-K list (STAGE_TOPK)
     uint64_t best;                     // argmax of leaf keys and fallbacks (STAGE_LEAF)
+    uint64_t best2;                    // the second-largest leaf key (tracing flavour only)
     uint32_t lo, hi;                   // TOPK: bit k = parent k has a legal child; LEAF: bit = list legal
 };
+
+// keep the two largest keys (keys are unique per move, 0 = none)
+__device__ __forceinline__ void top2_insert(uint64_t& b1, uint64_t& b2, uint64_t k) {
+    if (k > b1) {
+        b2 = b1;
+        b1 = k;
+    } else if (k > b2) {
+        b2 = k;
+    }
+}
+
+// the two largest keys over the warp, in every lane (each step merges disjoint lane sets)
+__device__ __forceinline__ void warp_top2(uint64_t& b1, uint64_t& b2) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        int const src = int((threadIdx.x + o) & 31u);
+        uint64_t const u1 = shfl64(b1, src), u2 = shfl64(b2, src);
+        uint64_t const lo = b1 < u1 ? b1 : u1, hi2 = b2 > u2 ? b2 : u2;
+        b1 = b1 > u1 ? b1 : u1;
+        b2 = lo > hi2 ? lo : hi2;
+    }
+}
 
 __device__ __forceinline__ uint64_t candidate_key(bool leaf, float v, uint32_t info, uint32_t i) {
     uint32_t const k = (info >> 8) & 31u, child = (info >> 21) & 1u;
@@ -518,12 +543,12 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality.
-template <int NET>
+template <int NET, bool KEYS>
 __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float* hb, bool leaf,
                                                uint32_t total, int kl, int lane, uint32_t& evals) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
-    LevelAcc acc{0, 0, 0, 0, 0};
+    LevelAcc acc{0, 0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
             ++evals;
@@ -533,8 +558,12 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
         }
     };
     auto fold = [&](uint64_t key) {
-        if (leaf) acc.best = key > acc.best ? key : acc.best;
-        else topk_fold(acc.list, acc.thr, key, kl, lane);
+        if (leaf) {
+            if (KEYS) top2_insert(acc.best, acc.best2, key);
+            else acc.best = key > acc.best ? key : acc.best;
+        } else {
+            topk_fold(acc.list, acc.thr, key, kl, lane);
+        }
     };
     auto drain = [&](uint32_t n, uint32_t queued) {
         uint64_t key = 0;
@@ -692,11 +721,11 @@ __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
 }
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
-template <int NET>
+template <int NET, bool KEYS>
 __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
     constexpr bool WIDE = NET != 0;
-    Move mv{0, 0, 0, true};
+    Move mv{0, 0, 0, true, 0, 0};
     if (ws.eng.over) return mv;
     uint32_t slot_piece[NSLOTS];                                  // beam.hpp:226-237
     slot_piece[0] = ws.eng.held;
@@ -710,6 +739,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     int kept = 1;                              // frontier size feeding the next stage
     uint32_t fscore = 0, fnode = 0, frank = uint32_t(lane), root_slot = 0;
     uint64_t best = 0;                         // leaf-order (score | order) maximum, fallbacks included
+    uint64_t best2 = 0;                        // the second-largest such key (tracing flavour)
 #pragma unroll 1
     for (int stage = 0; stage < DEPTH; ++stage) {
         bool const leaf = stage == DEPTH - 1;
@@ -735,8 +765,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
         // ---- every candidate of the stage
-        LevelAcc const a = level_pass<NET>(ws, lut, fw, hb, leaf, total, stage == 0 ? K0 : (stage == 1 ? K1 : K2),
-                                             lane, evals);
+        LevelAcc const a = level_pass<NET, KEYS>(ws, lut, fw, hb, leaf, total,
+                                                   stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane, evals);
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
             kept = __popc(__ballot_sync(FULL_MASK, a.list != 0));
@@ -751,7 +781,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             // kept nodes with no legal continuation become leaves at this depth (beam.hpp:549-551)
             if (lane < kept && !((has_child >> lane) & 1u)) {
                 uint64_t const fk = (uint64_t(fscore) << 32) | uint64_t(ORDER_SPAN - (LEAF_ORDERS + frank));
-                best = fk > best ? fk : best;
+                if (KEYS) top2_insert(best, best2, fk);
+                else best = fk > best ? fk : best;
             }
             int const next = __popc(__ballot_sync(FULL_MASK, a.list != 0));
             // advance the frontier (beam.hpp:379-403): lane j builds kept node j
@@ -771,7 +802,12 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
             // ---- leaf stage (beam.hpp:407-443): a list whose piece never fit scores the frontier board
             uint32_t const legal_lo = __reduce_or_sync(FULL_MASK, a.lo);
             uint32_t const legal_hi = __reduce_or_sync(FULL_MASK, a.hi);
-            best = a.best > best ? a.best : best;
+            if (KEYS) {
+                top2_insert(best, best2, a.best);
+                top2_insert(best, best2, a.best2);
+            } else {
+                best = a.best > best ? a.best : best;
+            }
 #pragma unroll
             for (int half = 0; half < 2; ++half) {
                 int const j = lane + 32 * half;
@@ -780,12 +816,19 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
                 bool const legal = ((half ? legal_hi : legal_lo) >> lane) & 1u;
                 if (k < kept && !legal) {
                     uint64_t const key = (uint64_t(sc) << 32) | uint64_t(ORDER_SPAN - uint32_t(j) * MP);
-                    best = key > best ? key : best;
+                    if (KEYS) top2_insert(best, best2, key);
+                    else best = key > best ? key : best;
                 }
             }
         }
     }
-    best = warp_max64(best);
+    if (KEYS) {
+        warp_top2(best, best2);
+        mv.key1 = best;
+        mv.key2 = best2;
+    } else {
+        best = warp_max64(best);
+    }
     if (best == 0) {                                              // unreachable with >= 1 root
         if (lane == 0) atomicOr(status, 1u);
         return mv;
@@ -808,7 +851,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
 // model, 32: 1,441) instead of v11.
 // BUDGET: the flavour that checks the launch's time budget after every move (a separate
 // instantiation: the check's registers would otherwise cost the ordinary kernels spills).
-template <int WARPS, int MINB, int NET = 0, bool BUDGET = false>
+// KEYS: the tracing flavour that also records each move's two largest final keys (p.keys).
+template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;
@@ -861,7 +905,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         __syncwarp();
         uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move<NET>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            Move const mv = search_move<NET, KEYS>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            if (KEYS && lane == 0 && p.keys) {
+                p.keys[(size_t(sim) * p.max_moves + moves) * 2] = mv.key1;
+                p.keys[(size_t(sim) * p.max_moves + moves) * 2 + 1] = mv.key2;
+            }
             if (mv.none) break;
             if (lane == 0) {
                 if (p.trace) {
@@ -988,6 +1036,10 @@ Variant const kWideNet[NUM_NETS] = {{nullptr, 0, 0}, {eval_kernel<4, 2, 64>, 4, 
 // the budget-checking flavours (shapes where the extra check spills nothing)
 Variant const kBudgetNet[NUM_NETS] = {{eval_kernel<4, 3, 0, true>, 4, 3}, {eval_kernel<4, 2, 64, true>, 4, 2},
                                       {eval_kernel<4, 3, 32, true>, 4, 3}};
+// the tracing flavours that record each move's two largest keys (without a time budget)
+Variant const kKeysNet[NUM_NETS] = {{eval_kernel<4, 3, 0, false, true>, 4, 3},
+                                    {eval_kernel<4, 2, 64, false, true>, 4, 2},
+                                    {eval_kernel<4, 3, 32, false, true>, 4, 3}};
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
@@ -1027,6 +1079,9 @@ struct ta3b_ctx {
     unsigned long long budget_ns = 0; // per-launch time budget (0 = none)
     uint32_t net_grid[NUM_NETS] = {0, 0, 0};     // widened-network kernels (by NetKind), set up on first use
     uint32_t budget_grid[NUM_NETS] = {0, 0, 0};  // budget flavours (by NetKind), set up on first use
+    uint32_t keys_grid[NUM_NETS] = {0, 0, 0};    // key-tracing flavours (by NetKind), set up on first use
+    uint64_t* d_keys = nullptr;                  // per move the two largest final keys (tracing)
+    size_t cap_keys = 0;
     uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
     std::string err;
 };
@@ -1137,14 +1192,22 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     if (prm.total_sims == 0) return TA3B_OK;
     if (ni != NET_V11 && !ctx->net_grid[ni])
         if (int rc = setup_kernel(ctx, kWideNet[ni], ni, ctx->net_grid[ni], "widened kernel")) return rc;
-    bool const budget = ctx->budget_ns != 0;
+    bool const keys = prm.keys != nullptr;
+    bool const budget = ctx->budget_ns != 0 && !keys;
     if (budget && !ctx->budget_grid[ni])
         if (int rc = setup_kernel(ctx, kBudgetNet[ni], ni, ctx->budget_grid[ni], "budget kernel")) return rc;
+    if (keys && !ctx->keys_grid[ni])
+        if (int rc = setup_kernel(ctx, kKeysNet[ni], ni, ctx->keys_grid[ni], "key-tracing kernel")) return rc;
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, kScratchBytes, st), "reset work queue");
-    // with a time budget the budget-checking flavour runs (its own fixed launch shape)
-    Variant const* const v = budget ? &kBudgetNet[ni] : ni != NET_V11 ? &kWideNet[ni] : &kVariants[ctx->variant];
+    // with a time budget the budget-checking flavour runs, with key tracing the tracing flavour
+    // (which runs without the budget); each has its own fixed launch shape
+    Variant const* const v = keys     ? &kKeysNet[ni]
+                             : budget ? &kBudgetNet[ni]
+                             : ni != NET_V11 ? &kWideNet[ni] : &kVariants[ctx->variant];
     uint32_t const warps = v->warps;
-    uint32_t const max_grid = budget ? ctx->budget_grid[ni] : ni != NET_V11 ? ctx->net_grid[ni] : ctx->grid;
+    uint32_t const max_grid = keys     ? ctx->keys_grid[ni]
+                              : budget ? ctx->budget_grid[ni]
+                              : ni != NET_V11 ? ctx->net_grid[ni] : ctx->grid;
     uint32_t const need_blocks = (prm.total_sims + warps - 1) / warps;
     uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
     Params p2 = prm;
@@ -1177,7 +1240,7 @@ int status_code(ta3b_ctx* ctx, uint32_t status) {
 int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_t mpi, uint32_t num_params,
               uint64_t const* seeds, uint32_t num_games, uint32_t max_moves, float* score_out, uint32_t* pieces_out,
               uint32_t* lines_out, uint32_t* evals_out, uint8_t* trace_out, uint32_t* nmoves_out,
-              uint32_t* board_out, uint64_t* timing_out = nullptr) {
+              uint32_t* board_out, uint64_t* timing_out = nullptr, uint64_t* keys_out = nullptr) {
     if (int rc = check_sizes(ctx, num_islands, mpi, num_params, num_games)) return rc;
     uint64_t const models = uint64_t(num_islands) * mpi;
     uint64_t const sims = models * num_games;
@@ -1197,7 +1260,9 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
         if (int rc = grow(ctx, ctx->d_evals, c, sims, "alloc evals")) return rc;
         ctx->cap_sims = sims;
     }
-    bool const tracing = trace_out || nmoves_out || board_out;
+    bool const tracing = trace_out || nmoves_out || board_out || keys_out;
+    if (keys_out)
+        if (int rc = grow(ctx, ctx->d_keys, ctx->cap_keys, sims * max_moves * 2 + 2, "alloc keys")) return rc;
     if (timing_out)
         if (int rc = grow(ctx, ctx->d_timing, ctx->cap_timing, 2 * sims, "alloc timing")) return rc;
     if (tracing) {
@@ -1234,6 +1299,7 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     prm.board_out = tracing ? ctx->d_board : nullptr;
     prm.scratch = ctx->d_scratch;
     prm.timing = timing_out ? reinterpret_cast<unsigned long long*>(ctx->d_timing) : nullptr;
+    prm.keys = keys_out ? reinterpret_cast<unsigned long long*>(ctx->d_keys) : nullptr;
     prm.num_games = num_games;
     prm.models_per_island = mpi;
     prm.max_moves = max_moves;
@@ -1262,6 +1328,9 @@ int host_eval(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_
     if (timing_out)
         TA3B_CUDA(ctx, cudaMemcpyAsync(timing_out, ctx->d_timing, sims * 16, cudaMemcpyDeviceToHost, ctx->stream),
                   "copy timing");
+    if (keys_out)
+        TA3B_CUDA(ctx, cudaMemcpyAsync(keys_out, ctx->d_keys, sims * max_moves * 16, cudaMemcpyDeviceToHost,
+                                       ctx->stream), "copy keys");
     return read_status(ctx);
 }
 
@@ -1348,7 +1417,8 @@ void ta3b_destroy(ta3b_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     void* bufs[] = {ctx->d_w, ctx->d_seeds, ctx->d_score, ctx->d_pieces, ctx->d_lines, ctx->d_evals,
-                    ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing, ctx->d_wpad};
+                    ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing, ctx->d_wpad,
+                    ctx->d_keys};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1373,9 +1443,9 @@ int ta3b_eval_islands(ta3b_ctx* ctx, float const* weights, uint32_t num_islands,
 int ta3b_eval_trace(ta3b_ctx* ctx, float const* weights, uint32_t num_models, uint32_t num_params,
                     uint64_t const* seeds, uint32_t num_games, uint32_t max_moves, float* score_out,
                     uint32_t* pieces_out, uint32_t* lines_out, uint32_t* evals_out, uint8_t* trace_out,
-                    uint32_t* n_moves_out, uint32_t* board_out) {
+                    uint32_t* n_moves_out, uint32_t* board_out, uint64_t* keys_out) {
     return host_eval(ctx, weights, 1, num_models, num_params, seeds, num_games, max_moves, score_out, pieces_out,
-                     lines_out, evals_out, trace_out, n_moves_out, board_out);
+                     lines_out, evals_out, trace_out, n_moves_out, board_out, nullptr, keys_out);
 }
 
 int ta3b_eval_timed(ta3b_ctx* ctx, float const* weights, uint32_t num_islands, uint32_t models_per_island,

@@ -62,7 +62,7 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_eval.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp]
     lib.ta3b_eval_islands.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp]
     lib.ta3b_eval_device.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp]
-    lib.ta3b_eval_trace.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp]
+    lib.ta3b_eval_trace.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp]
     lib.ta3b_eval_timed.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp]
     lib.ta3b_simulate_seeds.argtypes = [u64, u32, vp]
     lib.ta3b_launch_info.argtypes = [vp, vp, vp, vp]
@@ -90,6 +90,45 @@ def simulate_seeds(seed: int, games: int) -> np.ndarray:
     if rc:
         raise EvaluatorError("ta3b_simulate_seeds failed")
     return out
+
+
+# The final argmax of a move compares 64-bit keys (ta3_ai/incl/ta3/ai/search/beam.hpp:204-224):
+# high word = ordered_bits(value), a monotone map of the float's bits; low word = ORDER_SPAN - order,
+# so on equal values the lowest order wins. order < LEAF_ORDERS is a leaf (parent rank * 2 + child
+# list) * MAX_PLACEMENTS + placement; LEAF_ORDERS + rank is a frontier node with no child.
+ORDER_SPAN = 32 * 2 * 34 + 16
+LEAF_ORDERS = 32 * 2 * 34
+
+
+def ordered_bits_inv(s: int) -> np.float32:
+    """The float a key's high word encodes (beam.hpp:209-211)."""
+    s = int(s) & 0xFFFFFFFF
+    u = (s ^ 0x80000000) if s & 0x80000000 else (~s & 0xFFFFFFFF)
+    return np.array([u], np.uint32).view(np.float32)[0]
+
+
+def ordered_bits(v) -> int:
+    """beam.hpp:204-207: the monotone map of a float's bits."""
+    u = int(np.array([v], np.float32).view(np.uint32)[0])
+    return (~u & 0xFFFFFFFF) if u & 0x80000000 else (u | 0x80000000)
+
+
+def decode_key(key: int):
+    """(value, order) of a final-argmax key; (None, None) for the empty key 0."""
+    key = int(key)
+    if key == 0:
+        return None, None
+    return ordered_bits_inv(key >> 32), ORDER_SPAN - (key & 0xFFFFFFFF)
+
+
+def top2_margin(key1: int, key2: int):
+    """How far the chosen key's value lies above the runner-up's (float64 difference of the two
+    float32 values); None when the move had a single candidate."""
+    v1, _ = decode_key(key1)
+    v2, _ = decode_key(key2)
+    if v1 is None or v2 is None:
+        return None
+    return float(np.float64(v1) - np.float64(v2))
 
 
 class ModelEvaluator:
@@ -175,18 +214,22 @@ class ModelEvaluator:
                                               games, max_moves, _p(sc), _p(pc), _p(ec), _p(tm)))
         return sc, pc, ec, tm
 
-    def eval_trace(self, weights, num_models: int, seeds, max_moves: int):
-        """Everything, plus per-move traces: dict of model-major arrays."""
+    def eval_trace(self, weights, num_models: int, seeds, max_moves: int, keys: bool = False):
+        """Everything, plus per-move traces: dict of model-major arrays. keys=True adds
+        "keys" (sims, max_moves, 2) uint64: each searched move's two largest final keys
+        (decode with decode_key; see top2_margin)."""
         w, s = self._prep(weights, num_models, seeds)
         n = num_models * s.size
         out = {"score": np.zeros(n, np.float32), "pieces": np.zeros(n, np.uint32), "lines": np.zeros(n, np.uint32),
                "evals": np.zeros(n, np.uint32), "trace": np.zeros((n, max(max_moves, 1) * 3), np.uint8),
                "moves": np.zeros(n, np.uint32), "board": np.zeros((n, 10), np.uint32)}
+        if keys:
+            out["keys"] = np.zeros((n, max(max_moves, 1), 2), np.uint64)
         self._check(self._lib.ta3b_eval_trace(self._ctx, _p(w), num_models, self._nparams(w, num_models), _p(s), s.size,
                                               max_moves,
                                               _p(out["score"]), _p(out["pieces"]), _p(out["lines"]),
                                               _p(out["evals"]), _p(out["trace"]), _p(out["moves"]),
-                                              _p(out["board"])))
+                                              _p(out["board"]), _p(out.get("keys"))))
         return out
 
     def eval_device(self, weights, seeds, max_moves: int, score, pieces=None, lines=None, evals=None,
