@@ -74,6 +74,7 @@ typedef struct {
     uint32_t surrogate_batch;       /* built-in GPU surrogate: minibatch rows */
     double surrogate_lr;            /* built-in GPU surrogate: Adam learning rate */
     uint32_t surrogate_window;      /* train on the last N generations before the held-out one (0 = all) */
+    uint32_t num_devices;           /* built-in evaluator: island groups on devices device .. device + n - 1 */
 } ta3t_config;
 
 typedef struct {
@@ -102,6 +103,17 @@ void ta3t_default_config(ta3t_config* cfg);
  * surrogate_start_gen > 0: the built-in GPU surrogate (ta3b_surrogate.h).
  * NULL on failure (message via ta3t_last_error(NULL)). */
 ta3t_trainer* ta3t_create(const ta3t_config* cfg, ta3t_score_fn score_fn, void* user, const ta3t_surrogate* surrogate);
+/* Island groups (the multi-GPU split of a training run): islands i with
+ * i % num_groups == g are scored by score_fns[g] (with users[g]), every group
+ * on its own host thread, concurrently; the built-in evaluator does the same
+ * with one context per device when cfg->num_devices > 1 (ta3t_create). Every
+ * generation stays one lock-step step of all islands, and as the evaluator is
+ * deterministic a split run equals the single-device run bit for bit. The
+ * reference runs its islands on host threads with one evaluator per
+ * model-scheduler thread (ta3_trainer/src/trainer2.cpp:98-100,144-170,
+ * ta3_gpu/incl/ta3/gpu/model_eval.hpp:21-26). */
+ta3t_trainer* ta3t_create_groups(const ta3t_config* cfg, uint32_t num_groups, const ta3t_score_fn* score_fns,
+                                 void* const* users, const ta3t_surrogate* surrogate);
 /* Like ta3t_create, but every island's optimiser resumes from a saved state
  * (trainer2.cpp:178-212: the best island's optimiser, copied to all islands,
  * re-seeded per island). */

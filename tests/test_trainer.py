@@ -231,3 +231,50 @@ def test_corrupt_champ_files_are_rejected(host, tmp_path):
     p.write_bytes(b"\x01\x02")
     with pytest.raises(OSError):
         host.read_champ(str(p))
+
+
+class _Recorder:
+    """A fake device: the quadratic score, recording which rows it was given."""
+
+    def __init__(self):
+        self.rows = []
+
+    def __call__(self, w, seeds, max_moves):
+        self.rows.append(w.copy())
+        return quadratic(w, seeds, max_moves)
+
+
+def _final(t, islands):
+    return [t.champion(i) for i in range(islands)], [t.island_mean(i) for i in range(islands)]
+
+
+@pytest.mark.parametrize("groups", [2, 3])
+def test_island_groups_equal_the_single_device_run(host, groups):
+    """Islands split over `groups` fake devices (island i scored by device i % groups, the devices
+    on concurrent host threads) give the single-device run's champions and means bit for bit,
+    and each device sees only its own islands' candidates."""
+    cfg = dict(islands=4, population=8, gens_per_iteration=3, iterations_per_cycle=2, games=3, max_moves=50)
+    one = host.Trainer(small(host, **cfg), score=quadratic)
+    one.run(4)
+    devs = [_Recorder() for _ in range(groups)]
+    split = host.Trainer(small(host, **cfg), score=devs)
+    split.run(4)
+    (c1, m1), (c2, m2) = _final(one, 4), _final(split, 4)
+    for (x1, f1), (x2, f2) in zip(c1, c2):
+        assert f1 == f2 and x1.tobytes() == x2.tobytes()
+    assert all(a.tobytes() == b.tobytes() for a, b in zip(m1, m2))
+    assert one.stats()["evaluations"] == split.stats()["evaluations"]
+    # one generation = one call per device, each with its islands' rows (8 per island)
+    n_islands = [len(range(g, 4, groups)) for g in range(groups)]
+    for d, k in zip(devs, n_islands):
+        assert len(d.rows) == 1 + 4 * 3 and all(r.shape[0] == 8 * k for r in d.rows)
+
+
+def test_built_in_evaluator_groups_need_devices(host):
+    """num_devices > 1 asks the built-in evaluator for one context per device; without those
+    devices creation fails with the evaluator's error (no silent fallback)."""
+    import torch
+    if torch.cuda.is_available() and torch.cuda.device_count() >= 2:
+        pytest.skip("checks the missing-device error path")
+    with pytest.raises(RuntimeError, match="evaluator"):
+        host.Trainer(small(host, num_devices=2))

@@ -1,7 +1,18 @@
-"""Multi-GPU plumbing for the evaluation path: one process per GPU, each rank
-evaluates its own batch of sims (sims are independent, so there is no
-data-path collective); the only communication is the end-of-run reduction of
-device-timed seconds (max over ranks) and evaluated placements (sum)."""
+"""Multi-GPU plumbing, one process per GPU.
+
+Evaluation (bench.py): each rank evaluates its own batch of sims (sims are
+independent, so there is no data-path collective); the only communication is
+the end-of-run reduction of device-timed seconds (max over ranks) and evaluated
+placements (sum).
+
+Training (island_group_score): a training run splits its islands into groups,
+one per rank. Every rank keeps the whole (small) host state of the trainer --
+all islands' optimisers, in lock step -- but scores only its own islands'
+candidates; one all-gather of the per-game scores per generation then gives
+every rank the full generation, so all ranks take identical optimiser steps and
+the ring migration moves individuals between islands scored on different
+ranks. The reference runs its islands on host threads, one evaluator each
+(ta3_trainer/src/trainer2.cpp:98-100,144-170)."""
 from __future__ import annotations
 
 import os
@@ -30,3 +41,49 @@ def reduce_timing(seconds: float, units: float, device=None):
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     dist.all_reduce(u, op=dist.ReduceOp.SUM)
     return float(t.item()), float(u.item()), float(u.item()) / float(t.item())
+
+
+def island_group_score(local_score, islands: int, group=None):
+    """A trainer score function (weights (n, P) float32, seeds (G,), max_moves ->
+    scores (n, G), pieces (n, G)) for one rank of an island-group split: rows are
+    island-major (n / islands per island); this rank scores islands i with
+    i % world == rank through `local_score` and all-gathers the rest (the
+    process group `group`, default the world). Without a process group it is
+    `local_score` itself."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return local_score
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+
+    def score(w, seeds, max_moves):
+        n = w.shape[0]
+        if n % islands:
+            raise ValueError("rows must be island-major with equal rows per island")
+        rows, games = n // islands, len(seeds)
+        mine = [i for i in range(islands) if i % world == rank]
+        sc = np.zeros((n, games), np.float32)
+        pc = np.zeros((n, games), np.uint32)
+        if mine:
+            idx = np.concatenate([np.arange(i * rows, (i + 1) * rows) for i in mine])
+            res = local_score(np.ascontiguousarray(w[idx]), seeds, max_moves)
+            s, p = res if isinstance(res, tuple) else (res, np.zeros((idx.size, games), np.uint32))
+            sc[idx] = np.asarray(s, np.float32).reshape(idx.size, games)
+            pc[idx] = np.asarray(p, np.uint32).reshape(idx.size, games)
+        # each rank's islands' rows, bit patterns as int32; rank r's part supplies islands i % world == r
+        t = torch.from_numpy(np.concatenate([sc.view(np.int32), pc.view(np.int32)], axis=1))
+        parts = [torch.empty_like(t) for _ in range(world)]
+        dist.all_gather(parts, t, group=group)
+        full_s = np.zeros((n, games), np.int32)
+        full_p = np.zeros((n, games), np.int32)
+        for r, part in enumerate(parts):
+            a = part.numpy()
+            for i in range(islands):
+                if i % world == r:
+                    full_s[i * rows:(i + 1) * rows] = a[i * rows:(i + 1) * rows, :games]
+                    full_p[i * rows:(i + 1) * rows] = a[i * rows:(i + 1) * rows, games:]
+        return full_s.view(np.float32), full_p.view(np.uint32)
+
+    return score

@@ -174,11 +174,17 @@ struct Island {
 
 } // namespace
 
+// One island group's evaluator: islands i with i % groups == g are scored by group g's
+// score function, on its own host thread (the built-in one: its own GPU context).
+struct Group {
+    ta3t_score_fn fn = nullptr;
+    void* user = nullptr;
+    ta3b_ctx* gpu = nullptr;          // owned (built-in evaluator)
+};
+
 struct ta3t_trainer {
     ta3t_config cfg{};
-    ta3t_score_fn score_fn = nullptr;
-    void* user = nullptr;
-    ta3b_ctx* gpu = nullptr;
+    std::vector<Group> groups;
     std::unique_ptr<GpuSurrogate> gpu_sur;
     bool has_surrogate = false;
     ta3t_surrogate sur{};
@@ -196,7 +202,8 @@ struct ta3t_trainer {
     bool sur_active = false;
 
     ~ta3t_trainer() {
-        if (gpu) ta3b_destroy(gpu);
+        for (auto& g : groups)
+            if (g.gpu) ta3b_destroy(g.gpu);
     }
 
     int fail(std::string m) {
@@ -204,9 +211,10 @@ struct ta3t_trainer {
         return 1;
     }
 
-    // one evaluator call over n candidates (row-major doubles): fitness = -mean score
+    // Score n candidates (row-major doubles, island-major: n / islands rows per island):
+    // fitness = -mean score. One evaluator call per island group, the groups concurrently.
     int score(size_t n, double const* xs, double* fitness, float* mean_out) {
-        uint32_t const P = cfg.num_params, G = cfg.games;
+        uint32_t const P = cfg.num_params, G = cfg.games, I = cfg.islands;
         std::vector<float> w(n * P);
         for (size_t i = 0; i < n * P; ++i) w[i] = static_cast<float>(xs[i]);   // tetris_problem2.cpp:35-38
         std::vector<uint64_t> seeds(G);
@@ -214,9 +222,40 @@ struct ta3t_trainer {
         std::vector<float> sc(n * G);
         std::vector<uint32_t> pc(n * G);
         auto const t0 = clock_t_::now();
-        int const rc = score_fn(user, w.data(), uint32_t(n), P, seeds.data(), G, cfg.max_moves, sc.data(), pc.data());
+        size_t const D = groups.size();
+        std::vector<int> rcs(D, 0);
+        if (D == 1) {
+            rcs[0] = groups[0].fn(groups[0].user, w.data(), uint32_t(n), P, seeds.data(), G, cfg.max_moves, sc.data(),
+                                  pc.data());
+        } else {
+            // island group g: islands g, g + D, ...; its rows gathered, scored, scattered back
+            size_t const rows = n / I;
+            auto run = [&](size_t g) {
+                std::vector<uint32_t> isl;
+                for (uint32_t i = uint32_t(g); i < I; i += uint32_t(D)) isl.push_back(i);
+                size_t const m = isl.size() * rows;
+                if (m == 0) return;
+                std::vector<float> wg(m * P), sg(m * G);
+                std::vector<uint32_t> pg(m * G);
+                for (size_t k = 0; k < isl.size(); ++k)
+                    std::memcpy(&wg[k * rows * P], &w[isl[k] * rows * P], rows * P * sizeof(float));
+                rcs[g] = groups[g].fn(groups[g].user, wg.data(), uint32_t(m), P, seeds.data(), G, cfg.max_moves,
+                                      sg.data(), pg.data());
+                for (size_t k = 0; k < isl.size(); ++k) {
+                    std::memcpy(&sc[isl[k] * rows * G], &sg[k * rows * G], rows * G * sizeof(float));
+                    std::memcpy(&pc[isl[k] * rows * G], &pg[k * rows * G], rows * G * sizeof(uint32_t));
+                }
+            };
+            std::vector<std::thread> th;
+            for (size_t g = 1; g < D; ++g) th.emplace_back(run, g);
+            run(0);
+            for (auto& t : th) t.join();
+        }
         st.eval_seconds += seconds_since(t0);
-        if (rc) return fail(gpu ? std::string("evaluator: ") + ta3b_last_error(gpu) : "score function failed");
+        for (size_t g = 0; g < D; ++g)
+            if (rcs[g])
+                return fail(groups[g].gpu ? std::string("evaluator: ") + ta3b_last_error(groups[g].gpu)
+                                          : "score function failed (island group " + std::to_string(g) + ")");
         for (size_t m = 0; m < n; ++m) {
             double sum = 0.0;                                            // tetris_problem2.cpp:59-64
             for (uint32_t g = 0; g < G; ++g) sum += double(sc[m * G + g]);
@@ -232,8 +271,12 @@ struct ta3t_trainer {
 
     ta3t_surrogate sur_builtin{};
 
-    int init(ta3t_config const* c, ta3t_score_fn fn, void* u, ta3t_surrogate const* s, std::string const* state) {
+    // fns / users: one score function per island group (a NULL entry: the built-in GPU evaluator
+    // on device cfg.device + group)
+    int init(ta3t_config const* c, uint32_t num_groups, ta3t_score_fn const* fns, void* const* users,
+             ta3t_surrogate const* s, std::string const* state) {
         cfg = *c;
+        if (num_groups == 0 || num_groups > 64) return fail("ta3t_create: 1 to 64 island groups");
         if (cfg.islands == 0 || cfg.population < 5 || cfg.games == 0 || cfg.num_params == 0 ||
             cfg.gens_per_iteration == 0 || cfg.iterations_per_cycle == 0)
             return fail("ta3t_create: islands, games, num_params, gens and iterations must be positive, population >= 5");
@@ -264,15 +307,18 @@ struct ta3t_trainer {
             has_surrogate = true;
             sur = *s;
         }
-        if (fn) {
-            score_fn = fn;
-            user = u;
-        } else {
-            ta3b_config const gc{c->device, 0, 0};
-            gpu = ta3b_create(&gc);
-            if (!gpu) return fail(std::string("evaluator: ") + ta3b_last_error(nullptr));
-            score_fn = gpu_score;
-            user = gpu;
+        groups.resize(num_groups);
+        for (uint32_t g = 0; g < num_groups; ++g) {
+            if (fns && fns[g]) {
+                groups[g].fn = fns[g];
+                groups[g].user = users ? users[g] : nullptr;
+            } else {
+                ta3b_config const gc{c->device + int(g), 0, 0};
+                groups[g].gpu = ta3b_create(&gc);
+                if (!groups[g].gpu) return fail(std::string("evaluator: ") + ta3b_last_error(nullptr));
+                groups[g].fn = gpu_score;
+                groups[g].user = groups[g].gpu;
+            }
         }
         st.last_rho = 0.0 / 0.0;
         generator = Xoshiro(cfg.training_seed);
@@ -533,16 +579,17 @@ void ta3t_default_config(ta3t_config* c) {
     c->surrogate_batch = 256;
     c->surrogate_lr = 1e-3;
     c->surrogate_window = 0;
+    c->num_devices = 1;
 }
 
-static ta3t_trainer* create(const ta3t_config* cfg, std::string const* state, ta3t_score_fn fn, void* user,
-                            const ta3t_surrogate* s) {
+static ta3t_trainer* create(const ta3t_config* cfg, std::string const* state, uint32_t groups,
+                            ta3t_score_fn const* fns, void* const* users, const ta3t_surrogate* s) {
     if (!cfg) {
         g_create_err = "ta3t_create: null config";
         return nullptr;
     }
     auto* t = new ta3t_trainer;
-    if (t->init(cfg, fn, user, s, state)) {
+    if (t->init(cfg, groups, fns, users, s, state)) {
         g_create_err = t->err;
         delete t;
         return nullptr;
@@ -551,7 +598,25 @@ static ta3t_trainer* create(const ta3t_config* cfg, std::string const* state, ta
 }
 
 ta3t_trainer* ta3t_create(const ta3t_config* cfg, ta3t_score_fn score_fn, void* user, const ta3t_surrogate* s) {
-    return create(cfg, nullptr, score_fn, user, s);
+    // the built-in evaluator: one island group per device (cfg->num_devices, at least one)
+    uint32_t const groups = score_fn || !cfg || cfg->num_devices < 2 ? 1u : cfg->num_devices;
+    std::vector<ta3t_score_fn> fns(groups, score_fn);
+    std::vector<void*> users(groups, user);
+    return create(cfg, nullptr, groups, fns.data(), users.data(), s);
+}
+
+ta3t_trainer* ta3t_create_groups(const ta3t_config* cfg, uint32_t num_groups, const ta3t_score_fn* score_fns,
+                                 void* const* users, const ta3t_surrogate* s) {
+    if (num_groups == 0 || !score_fns) {
+        g_create_err = "ta3t_create_groups: need at least one score function";
+        return nullptr;
+    }
+    for (uint32_t g = 0; g < num_groups; ++g)
+        if (!score_fns[g]) {
+            g_create_err = "ta3t_create_groups: null score function";
+            return nullptr;
+        }
+    return create(cfg, nullptr, num_groups, score_fns, users, s);
 }
 
 ta3t_trainer* ta3t_create_from_state(const ta3t_config* cfg, const char* state_path, ta3t_score_fn score_fn,
@@ -562,7 +627,10 @@ ta3t_trainer* ta3t_create_from_state(const ta3t_config* cfg, const char* state_p
         return nullptr;
     }
     std::string const blob((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
-    return create(cfg, &blob, score_fn, user, s);
+    uint32_t const groups = score_fn || !cfg || cfg->num_devices < 2 ? 1u : cfg->num_devices;
+    std::vector<ta3t_score_fn> fns(groups, score_fn);
+    std::vector<void*> users(groups, user);
+    return create(cfg, &blob, groups, fns.data(), users.data(), s);
 }
 
 void ta3t_destroy(ta3t_trainer* t) { delete t; }

@@ -37,7 +37,7 @@ class TrainerConfig(C.Structure):
                 ("surrogate_top", C.c_uint32), ("surrogate_random", C.c_uint32),
                 ("surrogate_retrain", C.c_uint32), ("surrogate_min_rho", C.c_double),
                 ("surrogate_epochs", C.c_uint32), ("surrogate_batch", C.c_uint32), ("surrogate_lr", C.c_double),
-                ("surrogate_window", C.c_uint32)]
+                ("surrogate_window", C.c_uint32), ("num_devices", C.c_uint32)]
 
 
 class TrainerStats(C.Structure):
@@ -84,6 +84,7 @@ def host_library() -> C.CDLL:
         "ta3t_create": (vp, [C.POINTER(TrainerConfig), SCORE_FN, vp, C.POINTER(SurrogateStruct)]),
         "ta3t_create_from_state": (vp, [C.POINTER(TrainerConfig), C.c_char_p, SCORE_FN, vp,
                                         C.POINTER(SurrogateStruct)]),
+        "ta3t_create_groups": (vp, [C.POINTER(TrainerConfig), u32, vp, vp, C.POINTER(SurrogateStruct)]),
         "ta3t_destroy": (None, [vp]),
         "ta3t_last_error": (C.c_char_p, [vp]),
         "ta3t_next_game_seed": (i32, [vp]),
@@ -108,7 +109,7 @@ def host_library() -> C.CDLL:
 HOST_EXPORTS = ["ta3c_create", "ta3c_destroy", "ta3c_new_evolve", "ta3c_ask", "ta3c_last_dx", "ta3c_tell",
                 "ta3c_mean", "ta3c_sigma", "ta3c_axis_std", "ta3c_dim", "ta3c_save", "ta3c_load",
                 "ta3c_last_error", "ta3c_sym_eig", "ta3c_run_test_problem", "ta3t_default_config", "ta3t_create",
-                "ta3t_create_from_state", "ta3t_destroy", "ta3t_last_error", "ta3t_next_game_seed",
+                "ta3t_create_from_state", "ta3t_create_groups", "ta3t_destroy", "ta3t_last_error", "ta3t_next_game_seed",
                 "ta3t_run_generation", "ta3t_run_iteration", "ta3t_run", "ta3t_get_stats", "ta3t_champion",
                 "ta3t_island_mean", "ta3t_save_state", "ta3t_write_champ", "ta3t_read_champ"]
 
@@ -228,10 +229,12 @@ ScoreCallable = Callable[[np.ndarray, np.ndarray, int], "np.ndarray | tuple[np.n
 class Trainer:
     """The island CMA-ES trainer. `score(weights (n, P) float32, seeds (G,)
     uint64, max_moves) -> scores (n, G)` (optionally also pieces) replaces the
-    GPU evaluator when given; `surrogate` is any object with
-    `train(x, y)` and `predict(x) -> mean score`."""
+    GPU evaluator when given; a list of such functions splits the islands into
+    groups (island i to score[i % len(score)], the groups on concurrent host
+    threads); `surrogate` is any object with `train(x, y)` and
+    `predict(x) -> mean score`."""
 
-    def __init__(self, config: Optional[TrainerConfig] = None, score: Optional[ScoreCallable] = None,
+    def __init__(self, config: Optional[TrainerConfig] = None, score=None,
                  surrogate=None, state_path: Optional[str] = None, **overrides):
         self.lib = host_library()
         self.cfg = config if config is not None else default_config()
@@ -239,8 +242,9 @@ class Trainer:
             setattr(self.cfg, k, v)
         self._keep = []
         self.calls = []          # (num_models, num_games, max_moves) of every score call
+        groups = list(score) if isinstance(score, (list, tuple)) else None
         fn = SCORE_FN()
-        if score is not None:
+        if score is not None and groups is None:
             fn = SCORE_FN(self._wrap_score(score))
         self._keep.append(fn)
         sp = None
@@ -248,7 +252,13 @@ class Trainer:
             s = SurrogateStruct(None, TRAIN_FN(self._wrap_train(surrogate)), PREDICT_FN(self._wrap_predict(surrogate)))
             self._keep.append(s)
             sp = C.byref(s)
-        if state_path is None:
+        if groups is not None:
+            if state_path is not None:
+                raise ValueError("island groups start from fresh populations")
+            fns = (SCORE_FN * len(groups))(*[SCORE_FN(self._wrap_score(g)) for g in groups])
+            self._keep.append(fns)
+            self.h = self.lib.ta3t_create_groups(C.byref(self.cfg), len(groups), C.cast(fns, C.c_void_p), None, sp)
+        elif state_path is None:
             self.h = self.lib.ta3t_create(C.byref(self.cfg), fn, None, sp)
         else:
             self.h = self.lib.ta3t_create_from_state(C.byref(self.cfg), state_path.encode(), fn, None, sp)
