@@ -44,6 +44,10 @@ int ta3c_tell(ta3c_opt* opt, uint32_t k, const int32_t* idx, const double* fitne
 int ta3c_mean(const ta3c_opt* opt, double* out);
 double ta3c_sigma(const ta3c_opt* opt);
 int ta3c_axis_std(const ta3c_opt* opt, double* out);
+/* k points (row-major) in the coordinates of the current search distribution,
+ * the inverse of ask's sampling map (there the distribution is N(0, I)). No
+ * reference counterpart. */
+int ta3c_whiten(const ta3c_opt* opt, uint32_t k, const double* x, double* z_out);
 uint32_t ta3c_dim(const ta3c_opt* opt);
 
 /* Full adaptation state (paths, D, C, accumulated update, random engine) in a

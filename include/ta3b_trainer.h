@@ -137,6 +137,11 @@ int ta3t_get_stats(const ta3t_trainer* t, ta3t_stats* out);
 int ta3t_champion(const ta3t_trainer* t, uint32_t island, double* x_out, double* f_out);
 /* current CMA-ES mean of an island */
 int ta3t_island_mean(const ta3t_trainer* t, uint32_t island, double* x_out);
+/* n parameter vectors (row-major) in an island's own search coordinates: the map
+ * under which its current sampling distribution is N(0, I) (dd-CMA-ES:
+ * z = C^(-1/2) ((x - m) / (sigma d)); sep-CMA-ES: (x - m) / (sigma sqrt(diag))).
+ * No reference counterpart (used to fit per-island surrogates). */
+int ta3t_island_whiten(const ta3t_trainer* t, uint32_t island, const double* x, uint32_t n, double* z_out);
 
 /* Trainer2::saveState (trainer2.cpp:213-268): the best island's optimiser state
  * to state_path, its champion to the same path with extension .champ */

@@ -132,3 +132,23 @@ def test_nan_fitness_ranks_last(host):
     a.tell(g)
     b.tell(f2)
     assert np.allclose(a.mean, b.mean)
+
+
+@pytest.mark.parametrize("kind", ["SEP", "DD"])
+def test_whiten_maps_samples_to_a_standard_normal(host, kind):
+    """Whitening inverts ask's sampling map: after some adaptation (an anisotropic, rotated
+    distribution for dd-CMA-ES), a large sample is N(0, I) in the whitened coordinates."""
+    import numpy as np
+    dim = 10
+    rng = np.random.default_rng(1)
+    rot = np.linalg.qr(rng.normal(size=(dim, dim)))[0]
+    scale = np.logspace(0, 2, dim)
+    opt = host.Cma(getattr(host, kind), np.full(dim, 0.5), np.full(dim, -5.0), np.full(dim, 5.0), 0.5, 7)
+    for _ in range(30):                                   # rotated ellipsoid: the distribution adapts
+        x = opt.ask(12)
+        f = (((x @ rot) * scale) ** 2).sum(1)
+        opt.tell(f)
+    x = opt.ask(20000)
+    z = opt.whiten(x)
+    assert np.abs(z.mean(0)).max() < 0.05
+    assert np.abs(np.cov(z.T) - np.eye(dim)).max() < 0.08

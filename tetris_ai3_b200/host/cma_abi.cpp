@@ -127,6 +127,12 @@ int ta3c_axis_std(const ta3c_opt* opt, double* out) {
     return 0;
 }
 
+int ta3c_whiten(const ta3c_opt* opt, uint32_t k, const double* x, double* z_out) {
+    if (!opt || (k && (!x || !z_out))) return fail("ta3c_whiten: null argument");
+    opt->cma->whiten(int(k), x, z_out);
+    return 0;
+}
+
 uint32_t ta3c_dim(const ta3c_opt* opt) { return opt ? uint32_t(opt->cma->dim()) : 0u; }
 
 uint64_t ta3c_save(const ta3c_opt* opt, void* buf, uint64_t cap) {

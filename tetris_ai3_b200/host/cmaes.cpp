@@ -219,6 +219,14 @@ vec SepCma::axis_std() const {
     return s;
 }
 
+void SepCma::whiten(int k, double const* x, double* z) const {
+    // ask: x = m + sigma * sqrt(diag) * z
+    vec const s = axis_std();
+    for (int i = 0; i < k; ++i)
+        for (int j = 0; j < n_; ++j)
+            z[size_t(i) * n_ + j] = (x[size_t(i) * n_ + j] - mean_[size_t(j)]) / s[size_t(j)];
+}
+
 void SepCma::ask(int lam, double* out) {
     // sep_cmaes.cpp:170-178: per candidate, n normal draws, x = m + sigma * sqrt(diag) * z
     axis_.resize(static_cast<size_t>(n_));
@@ -405,6 +413,16 @@ vec DdCma::axis_std() const {
     vec s(static_cast<size_t>(n_));
     for (int j = 0; j < n_; ++j) s[size_t(j)] = sigma_ * d_[size_t(j)] * std::sqrt(corr_(j, j));
     return s;
+}
+
+void DdCma::whiten(int k, double const* x, double* z) const {
+    // ask: x = m + (sigma d) * sqrtC z, so z = C^(-1/2) ((x - m) / (sigma d))
+    vec y(static_cast<size_t>(n_));
+    for (int i = 0; i < k; ++i) {
+        for (int j = 0; j < n_; ++j)
+            y[size_t(j)] = (x[size_t(i) * n_ + j] - mean_[size_t(j)]) / (sigma_ * d_[size_t(j)]);
+        mat_vec(inv_sqrt_c_, y.data(), z + size_t(i) * n_);
+    }
 }
 
 void DdCma::ask(int lam, double* out) {

@@ -68,6 +68,9 @@ public:
     virtual double sigma() const = 0;
     // per-axis standard deviation of the current search distribution
     virtual vec axis_std() const = 0;
+    // k points (row-major) in the coordinates of the current search distribution: the map
+    // under which it is N(0, I), i.e. the inverse of ask's x = m + sigma * A z
+    virtual void whiten(int k, double const* x, double* z) const = 0;
     // Full adaptation state incl. the random engine and the normal
     // distribution's cached deviate: a restored optimiser continues identically.
     virtual std::string save() const = 0;
@@ -93,6 +96,7 @@ public:
     void tell(int k, int const* idx, double const* fitness) override;
     double sigma() const override { return sigma_; }
     vec axis_std() const override;
+    void whiten(int k, double const* x, double* z) const override;
     std::string save() const override;
     bool restore(std::string const& blob, size_t pos);
 
@@ -115,6 +119,7 @@ public:
     void tell(int k, int const* idx, double const* fitness) override;
     double sigma() const override { return sigma_; }
     vec axis_std() const override;
+    void whiten(int k, double const* x, double* z) const override;
     std::string save() const override;
     bool restore(std::string const& blob, size_t pos);
 

@@ -671,6 +671,12 @@ int ta3t_champion(const ta3t_trainer* t, uint32_t island, double* x_out, double*
     return 0;
 }
 
+int ta3t_island_whiten(const ta3t_trainer* t, uint32_t island, const double* x, uint32_t n, double* z_out) {
+    if (!t || island >= t->islands.size() || (n && (!x || !z_out))) return 1;
+    t->islands[island].cma->whiten(int(n), x, z_out);
+    return 0;
+}
+
 int ta3t_island_mean(const ta3t_trainer* t, uint32_t island, double* x_out) {
     if (!t || island >= t->islands.size() || !x_out) return 1;
     auto const& m = t->islands[island].cma->mean();

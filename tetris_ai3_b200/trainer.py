@@ -74,6 +74,7 @@ def host_library() -> C.CDLL:
         "ta3c_mean": (i32, [vp, vp]),
         "ta3c_sigma": (dbl, [vp]),
         "ta3c_axis_std": (i32, [vp, vp]),
+        "ta3c_whiten": (i32, [vp, u32, vp, vp]),
         "ta3c_dim": (u32, [vp]),
         "ta3c_save": (u64, [vp, vp, u64]),
         "ta3c_load": (vp, [vp, u64]),
@@ -94,6 +95,7 @@ def host_library() -> C.CDLL:
         "ta3t_get_stats": (i32, [vp, C.POINTER(TrainerStats)]),
         "ta3t_champion": (i32, [vp, u32, vp, vp]),
         "ta3t_island_mean": (i32, [vp, u32, vp]),
+        "ta3t_island_whiten": (i32, [vp, u32, vp, u32, vp]),
         "ta3t_save_state": (i32, [vp, C.c_char_p]),
         "ta3t_write_champ": (i32, [C.c_char_p, vp, u64]),
         "ta3t_read_champ": (u64, [C.c_char_p, vp, u64]),
@@ -107,11 +109,11 @@ def host_library() -> C.CDLL:
 
 
 HOST_EXPORTS = ["ta3c_create", "ta3c_destroy", "ta3c_new_evolve", "ta3c_ask", "ta3c_last_dx", "ta3c_tell",
-                "ta3c_mean", "ta3c_sigma", "ta3c_axis_std", "ta3c_dim", "ta3c_save", "ta3c_load",
+                "ta3c_mean", "ta3c_sigma", "ta3c_axis_std", "ta3c_whiten", "ta3c_dim", "ta3c_save", "ta3c_load",
                 "ta3c_last_error", "ta3c_sym_eig", "ta3c_run_test_problem", "ta3t_default_config", "ta3t_create",
                 "ta3t_create_from_state", "ta3t_create_groups", "ta3t_destroy", "ta3t_last_error", "ta3t_next_game_seed",
                 "ta3t_run_generation", "ta3t_run_iteration", "ta3t_run", "ta3t_get_stats", "ta3t_champion",
-                "ta3t_island_mean", "ta3t_save_state", "ta3t_write_champ", "ta3t_read_champ"]
+                "ta3t_island_mean", "ta3t_island_whiten", "ta3t_save_state", "ta3t_write_champ", "ta3t_read_champ"]
 
 
 def _p(a: np.ndarray):
@@ -170,6 +172,13 @@ class Cma:
         out = np.empty(self.dim)
         self._ok(self.lib.ta3c_axis_std(self.h, _p(out)))
         return out
+
+    def whiten(self, x) -> np.ndarray:
+        """Points (k, dim) in the coordinates where the current search distribution is N(0, I)."""
+        x = np.ascontiguousarray(np.atleast_2d(x), np.float64)
+        z = np.empty_like(x)
+        self._ok(self.lib.ta3c_whiten(self.h, x.shape[0], _p(x), _p(z)))
+        return z
 
     @property
     def last_dx(self) -> float:
@@ -341,6 +350,14 @@ class Trainer:
         x = np.empty(self.cfg.num_params)
         self._ok(self.lib.ta3t_island_mean(self.h, island, _p(x)))
         return x
+
+    def island_whiten(self, island: int, x) -> np.ndarray:
+        """Parameter vectors (n, P) in the island's own search coordinates (its sampling
+        distribution is N(0, I) there)."""
+        x = np.ascontiguousarray(np.atleast_2d(x), np.float64)
+        z = np.empty_like(x)
+        self._ok(self.lib.ta3t_island_whiten(self.h, island, _p(x), x.shape[0], _p(z)))
+        return z
 
     def save_state(self, path: str):
         self._ok(self.lib.ta3t_save_state(self.h, path.encode()))
