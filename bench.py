@@ -330,9 +330,11 @@ def run_ours(args):
                 "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz {sm_mhz:.0f} "
                                f"(MEASURED_PEAKS.json, {kind})",
                 "ops_per_placement": ops_per_placement,
-                "ops_basis": "reference algorithm per-placement operation count (hand count above)",
+                "ops_basis": "frac (the headline) counts the reference algorithm's operations per placement "
+                             "(an algorithmic count, hand count above); frac_executed counts the lane-instructions "
+                             "this kernel executes per placement (ncu thread_inst_executed / placements)",
                 "lane_instr_per_placement_measured": None if wide else LANE_INSTR_PER_PLACEMENT,
-                "issue_frac_measured": None if wide else per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12 / peak_issue}
+                "frac_executed": None if wide else per_gpu * LANE_INSTR_PER_PLACEMENT / 1e12 / peak_issue}
         if wide:
             roof["traffic"] = None
         cpu = None
