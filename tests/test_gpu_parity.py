@@ -223,10 +223,14 @@ def test_device_core_matches_host_core(ev):
             mism.append(("full", t, p, i, lg, int(ul[t]), v2.value, float(uv[t])))
     for m in mism[:8]:
         print("MISMATCH", m)
-    # the packed PTX f32x2 arithmetic (diagnostic slot 31) must give the same bits where the path evaluates
-    packed_bad = int(((fs == 0) & (dd[:, 31].view(np.uint32) != fv.view(np.uint32))).sum())
-    print("packed f32x2 MLP mismatches:", packed_bad, "of", int((fs == 0).sum()))
+    # every MLP arithmetic mode (scalar, packed PTX f32x2, packed intrinsics: diagnostic slots 29-31)
+    # gives the kernel's bits where the fast path evaluates
+    ok = fs == 0
+    bad = {name: int((ok & (dd[:, slot].view(np.uint32) != fv.view(np.uint32))).sum())
+           for name, slot in (("scalar", 29), ("packed intrinsics", 30), ("packed PTX", 31))}
+    print("MLP mode mismatches:", bad, "of", int(ok.sum()))
     assert not mism, f"{len(mism)} of {n} candidates differ"
+    assert sum(bad.values()) == 0, bad
 
 
 def test_generation_graph_replays_match_direct_calls(ev):

@@ -551,8 +551,10 @@ struct RecView {
 // Returns FAST_DEFER when a piece cell may meet the stack inside the spawn rows
 // or a row completes; the value is then meaningless.
 // MLP arithmetic: MLP_SCALAR = __fmul_rn / __fadd_rn per hidden unit;
-// MLP_PTX_X2 = pairs of hidden units per packed PTX instruction (mul/add.rn.f32x2).
-enum MlpMode { MLP_SCALAR = 0, MLP_PTX_X2 = 1 };
+// MLP_PTX_X2 = pairs of hidden units per packed PTX instruction (mul/add.rn.f32x2);
+// MLP_X2 = the same pairs through the __fmul2_rn / __fadd2_rn intrinsics. The packed
+// forms round each half exactly like the scalar .rn operation (checked on the device).
+enum MlpMode { MLP_SCALAR = 0, MLP_PTX_X2 = 1, MLP_X2 = 2 };
 
 // The fast path's features of one placement (holes, hole depths, surface,
 // wells, max height) from the parent record alone; true when the candidate
@@ -628,7 +630,14 @@ TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& 
 #pragma unroll
     for (int q = 0; q < NHID / 2; ++q) {
         float2 a = make_float2(r.P[2 * q], r.P[2 * q + 1]);
-        if (MLP == MLP_PTX_X2) {
+        if (MLP == MLP_X2) {
+            a = f2_add(a, f2_mul(x4, fw.w4[q]));
+            a = f2_add(a, f2_mul(x5, fw.w5[q]));
+            a = f2_add(a, f2_mul(x6, fw.w6[q]));
+            a = f2_add(a, f2_mul(x7, fw.w7[q]));
+            a = f2_add(a, f2_mul(x8, fw.w8[q]));
+            a = f2_add(a, f2_mul(x9, fw.w9[q]));
+        } else if (MLP == MLP_PTX_X2) {
             a = p2_add(a, p2_mul(x4, fw.w4[q]));
             a = p2_add(a, p2_mul(x5, fw.w5[q]));
             a = p2_add(a, p2_mul(x6, fw.w6[q]));
@@ -655,8 +664,9 @@ TA3B_HD int fast_eval(RecView const& r, PlaceFast pf, bool held_i, FastW const& 
         }
         a.x = a.x > 0.0f ? a.x : 0.0f;                      // std::max<float>(0, v)
         a.y = a.y > 0.0f ? a.y : 0.0f;
-        float2 const t = MLP == MLP_PTX_X2 ? p2_mul(a, fw.u[q]) : make_float2(f_mul(a.x, fw.u[q].x),
-                                                                              f_mul(a.y, fw.u[q].y));
+        float2 const t = MLP == MLP_PTX_X2 ? p2_mul(a, fw.u[q])
+                         : MLP == MLP_X2   ? f2_mul(a, fw.u[q])
+                                           : make_float2(f_mul(a.x, fw.u[q].x), f_mul(a.y, fw.u[q].y));
         v = f_add(v, t.x);
         v = f_add(v, t.y);
     }

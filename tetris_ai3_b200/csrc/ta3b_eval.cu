@@ -1265,11 +1265,15 @@ __global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand,
     FastW fw;
     load_fast_weights(GlobalW{w}, fw);
     float v = 0.0f;
-    // the kernel's own arithmetic mode, then (diagnostics only) the packed-PTX mode
+    // the kernel's own arithmetic mode, then (diagnostics) the other two: all must agree bit for bit
     fast_st[t] = fast_candidate(rec, g_lut.fast[piece][i], held, fw, v, dbg ? dbg + size_t(t) * 32 : nullptr);
     if (dbg) {
-        float v2 = 0.0f;
+        float v2 = 0.0f, v3 = 0.0f, v4 = 0.0f;
         fast_candidate<MLP_PTX_X2>(rec, g_lut.fast[piece][i], held, fw, v2, nullptr);
+        fast_candidate<MLP_X2>(rec, g_lut.fast[piece][i], held, fw, v3, nullptr);
+        fast_candidate<MLP_SCALAR>(rec, g_lut.fast[piece][i], held, fw, v4, nullptr);
+        dbg[size_t(t) * 32 + 29] = v4;
+        dbg[size_t(t) * 32 + 30] = v3;
         dbg[size_t(t) * 32 + 31] = v2;
     }
     fast_v[t] = v;
