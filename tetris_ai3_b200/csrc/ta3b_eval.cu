@@ -222,6 +222,9 @@ __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uin
     b[8] = q2.x; b[9] = q2.y;
 }
 
+#ifndef TA3B_ILP
+#define TA3B_ILP 1
+#endif
 #ifndef TA3B_MLP_MODE
 #define TA3B_MLP_MODE MLP_SCALAR
 #endif
@@ -426,144 +429,6 @@ __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
     return v;
 }
 
-// ----------------------------------------------------------------- teams ---
-// The launch's tail: once the work queue is empty, a warp that finishes its last
-// sim helps a game still running in its block instead of going idle. The game's
-// warp (the owner) admits helpers at move boundaries; from then on every stage's
-// flattened candidate space is dealt out across the team in 32-candidate rounds
-// (member r takes rounds r, r + T, ...), each member keeps its own top-K list /
-// argmax / legality bits, and the owner merges them. Keys are unique within a
-// stage, so the merged top-K and argmax are exactly the single-warp ones: a
-// team plays the same game, only sooner. Everything else of a move (records,
-// segments, decode, commit) stays with the owner.
-//
-// Synchronisation is a barrier in shared memory that the owner releases; every
-// wait gives up after kTeamWaitNs (no legitimate wait comes near it): the warp
-// sets status bit STATUS_TEAM and leaves, and the call reports TA3B_ERR_DEVICE.
-constexpr uint32_t kMaxTeam = 16;                            // members, owner included
-constexpr uint32_t TEAM_CLOSED = 0u, TEAM_OPEN = 1u;
-constexpr uint32_t CMD_RELEASE = 0xFFFFFFFFu;                // the game is over: helpers leave
-// join slot: requesting warp + 1 (bits 0-7), flags, member index << 16
-constexpr uint32_t JOIN_ADMIT = 0x100u, JOIN_WITHDRAWN = 0x200u;
-constexpr unsigned long long kTeamWaitNs = 1000000000ull;    // 1 s
-constexpr uint32_t STATUS_TEAM = 4u;
-// exchange words a helper leaves after a stage, in its own (unused) record area
-constexpr int X_BEST = 32, X_BITS = 33, X_EVALS = 34;
-
-struct TeamState {                     // in the owner's WarpShared
-    uint32_t state;                    // TEAM_OPEN while the owner's game accepts helpers
-    uint32_t req;                      // join slots reserved so far
-    uint32_t size;                     // members, owner included (written by the owner between moves)
-    uint32_t cmd;                      // the stage to run (0..3) or CMD_RELEASE
-    uint32_t broken;                   // owner: a team wait ran out, the game is abandoned
-    uint32_t total;                    // the stage's candidate count
-    uint32_t count, phase;             // the barrier
-    uint32_t scan;                     // owner: the next join slot to look at
-    uint32_t join[kMaxTeam - 1];
-    uint32_t member[kMaxTeam - 1];     // member k's warp (k = 1 .. size - 1) at member[k - 1]
-    uint32_t pad_;
-};
-static_assert(sizeof(TeamState) % 16 == 0, "team state keeps 16-byte alignment");
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// The team barrier: the owner releases it. Members arrive (count) and wait for the phase to
-// move; the owner waits until its size - 1 helpers have arrived, resets the count and moves
-// the phase. Only the owner needs the team's size, which it alone changes (between moves),
-// so a member admitted just before a barrier is counted exactly there. Writes before a
-// barrier are visible after it (fences around the arrival and the release). Every wait gives
-// up after kTeamWaitNs: false, with status bit STATUS_TEAM set.
-__device__ __forceinline__ bool team_sync_owner(TeamState* ts, uint32_t size, uint32_t* status, int lane) {
-    int ok = 1;
-    __syncwarp();
-    if (lane == 0) {
-        __threadfence_block();
-        volatile uint32_t* const vcount = &ts->count;
-        unsigned long long const t0 = global_ns();
-        while (*vcount != size - 1u) {
-            __nanosleep(16);
-            if (global_ns() - t0 > kTeamWaitNs) {
-                atomicOr(status, STATUS_TEAM);
-                ok = 0;
-                break;
-            }
-        }
-        __threadfence_block();
-        *vcount = 0u;
-        __threadfence_block();
-        atomicAdd(&ts->phase, 1u);                               // release
-    }
-    ok = __shfl_sync(FULL_MASK, ok, 0);
-    __syncwarp();
-    return ok != 0;
-}
-
-__device__ __forceinline__ bool team_sync_member(TeamState* ts, uint32_t* status, int lane) {
-    int ok = 1;
-    __syncwarp();
-    if (lane == 0) {
-        volatile uint32_t* const vph = &ts->phase;
-        uint32_t const ph = *vph;                                // cannot move before this warp arrives
-        __threadfence_block();
-        atomicAdd(&ts->count, 1u);
-        unsigned long long const t0 = global_ns();
-        while (*vph == ph) {
-            __nanosleep(32);
-            if (global_ns() - t0 > kTeamWaitNs) {
-                atomicOr(status, STATUS_TEAM);
-                ok = 0;
-                break;
-            }
-        }
-        __threadfence_block();
-    }
-    ok = __shfl_sync(FULL_MASK, ok, 0);
-    __syncwarp();
-    return ok != 0;
-}
-
-// owner, at a move boundary: admit the posted join requests in slot order (team size in ts->size)
-__device__ __forceinline__ void team_admit(TeamState* ts, int lane) {
-    if (lane == 0) {
-        uint32_t const req = *reinterpret_cast<volatile uint32_t*>(&ts->req);
-        uint32_t scan = ts->scan;
-        uint32_t size = ts->size;
-        while (scan < req && scan < kMaxTeam - 1 && size < kMaxTeam) {
-            uint32_t const v = *reinterpret_cast<volatile uint32_t*>(&ts->join[scan]);
-            if (v == 0) break;                                   // reserved, not yet posted
-            if (!(v & JOIN_WITHDRAWN) && atomicCAS(&ts->join[scan], v, v | JOIN_ADMIT | (size << 16)) == v) {
-                ts->member[size - 1] = (v & 0xFFu) - 1u;
-                ++size;
-            }
-            ++scan;
-        }
-        ts->scan = scan;
-        ts->size = size;
-        __threadfence_block();
-    }
-    __syncwarp();
-}
-
-// Bitonic merge of two descending 32-key lists (lane i = i-th largest) into the top kl keys.
-__device__ __forceinline__ uint64_t shfl64_xor(uint64_t v, int m) {
-    return (uint64_t(__shfl_xor_sync(FULL_MASK, uint32_t(v >> 32), m)) << 32) | __shfl_xor_sync(FULL_MASK, uint32_t(v), m);
-}
-__device__ __forceinline__ uint64_t merge_topk(uint64_t a, uint64_t b, int kl, int lane) {
-    uint64_t const rb = shfl64(b, 31 - lane);                    // ascending
-    uint64_t c = a > rb ? a : rb;                                // bitonic, holds the 32 largest of both
-#pragma unroll
-    for (int j = 16; j > 0; j >>= 1) {
-        uint64_t const o = shfl64_xor(c, j);
-        bool const lower = (lane & j) == 0;
-        c = lower ? (c > o ? c : o) : (c < o ? c : o);
-    }
-    return lane < kl ? c : 0ull;
-}
-
 // ---------------------------------------------------------------- kernel ---
 struct alignas(16) WarpShared {
     uint32_t rec[33][REC_WORDS];      // kept frontier records (rank -> record); [32] = committed board
@@ -575,7 +440,6 @@ struct alignas(16) WarpShared {
     uint32_t seg_off[65];              // a level's candidate segments (parent rank, child list)
     uint32_t seg_info[64];             // rec (6) | rank k << 8 | piece << 16 | held-is-I << 20 | child << 21
     uint32_t defer[64];                // queued (segment << 8 | placement) for the full path
-    TeamState team;                    // this warp's game's helpers (team kernels)
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte alignment");
 
@@ -678,14 +542,10 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // One level: every candidate of the segment table, on the fast path or queued
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
-// per-parent legality. ws is the game's (its records, segments and weights),
-// defer this warp's own queue; the warp takes the 32-candidate rounds first,
-// first + step, ... (first = 0, step = 32 alone; a team member r of T takes 32r,
-// step 32T).
+// per-parent legality.
 template <int NET, bool KEYS>
-__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* defer, Luts lut, FastW const& fw, float* hb,
-                                               bool leaf, uint32_t total, int kl, int lane, uint32_t& evals,
-                                               uint32_t first, uint32_t step) {
+__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float* hb, bool leaf,
+                                               uint32_t total, int kl, int lane, uint32_t& evals) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
     LevelAcc acc{0, 0, 0, 0, 0, 0};
@@ -713,7 +573,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* defer, 
             uint32_t entry = 0;
             bool legal = false;
             if (uint32_t(lane) < n) {
-                entry = defer[lane];
+                entry = ws.defer[lane];
                 legal = full_inputs_wide(&ws, lut, entry, in);
                 if (!legal) in = WideIn{};
             }
@@ -725,7 +585,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* defer, 
                 consume(key, entry >> 8, info);
             }
         } else if (uint32_t(lane) < n) {
-            uint32_t const entry = defer[lane];
+            uint32_t const entry = ws.defer[lane];
             key = full_key(&ws, lut, leaf, entry);
             consume(key, entry >> 8, ws.seg_info[entry >> 8]);
         }
@@ -733,44 +593,59 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* defer, 
         uint32_t const rem = queued - n;
         uint32_t t = 0;
         __syncwarp();
-        if (uint32_t(lane) < rem) t = defer[n + lane];
+        if (uint32_t(lane) < rem) t = ws.defer[n + lane];
         __syncwarp();
-        if (uint32_t(lane) < rem) defer[lane] = t;
+        if (uint32_t(lane) < rem) ws.defer[lane] = t;
         __syncwarp();
     };
     uint32_t queued = 0;
     int seg = 0;
-    // one candidate per lane per round (two per lane in straight-line code measured slower on
-    // B200: 681 ms per full-generation step vs 486 ms, no spills at 16 warps per SM)
-    for (uint32_t c0 = first; c0 < total; c0 += step) {
-        uint32_t const c = c0 + uint32_t(lane);
-        bool const valid = c < total;
-        uint32_t const cc = valid ? c : total - 1u;              // out of range: the last candidate, discarded
-        while (ws.seg_off[seg + 1] <= cc) ++seg;
-        uint32_t const sg = uint32_t(seg);
-        uint32_t const info = ws.seg_info[seg];
-        uint32_t const idx = cc - ws.seg_off[seg];
-        float v;
-        int st;
-        if constexpr (WIDE)
-            st = fast_candidate_wide<HW>(ws.rec[info & 63u], lut.fast[(info >> 16) & 7u][idx], (info >> 20) & 1u,
-                                         ws.wglobal, hb, lane, v);
-        else
-            st = fast_candidate(ws.rec[info & 63u], lut.fast[(info >> 16) & 7u][idx], (info >> 20) & 1u, fw, v);
-        uint64_t key = 0;
-        bool const def = valid && st != FAST_OK;
-        if (valid && st == FAST_OK) {
-            key = candidate_key(leaf, v, info, idx);
-            consume(key, sg, info);
+    // TA3B_ILP candidates per lane per iteration (c, c+32, ...) in straight-line
+    // code, so their dependency chains interleave; out-of-range slots evaluate
+    // the last real candidate and are discarded. 1 measured fastest on B200: 486 ms
+    // per full-generation step vs 681 ms for 2 (no spills at 16 warps per SM) and
+    // 766 ms for 2 at 12 warps per SM.
+    for (uint32_t c0 = 0; c0 < total; c0 += TA3B_ILP * WARP) {
+        uint32_t info[TA3B_ILP], idx[TA3B_ILP], sg[TA3B_ILP];
+        bool valid[TA3B_ILP];
+#pragma unroll
+        for (int u = 0; u < TA3B_ILP; ++u) {
+            uint32_t const c = c0 + uint32_t(u * WARP + lane);
+            valid[u] = c < total;
+            uint32_t const cc = valid[u] ? c : total - 1u;
+            while (ws.seg_off[seg + 1] <= cc) ++seg;
+            sg[u] = uint32_t(seg);
+            info[u] = ws.seg_info[seg];
+            idx[u] = cc - ws.seg_off[seg];
         }
-        uint32_t const dm = __ballot_sync(FULL_MASK, def);
-        if (def) defer[queued + __popc(dm & ((1u << lane) - 1u))] = (sg << 8) | idx;
-        queued += __popc(dm);
-        fold(key);
-        if (queued >= uint32_t(WARP)) {
-            __syncwarp();
-            drain(WARP, queued);
-            queued -= WARP;
+        float v[TA3B_ILP];
+        int st[TA3B_ILP];
+#pragma unroll
+        for (int u = 0; u < TA3B_ILP; ++u) {
+            if constexpr (WIDE)
+                st[u] = fast_candidate_wide<HW>(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
+                                                (info[u] >> 20) & 1u, ws.wglobal, hb, lane, v[u]);
+            else
+                st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
+                                       (info[u] >> 20) & 1u, fw, v[u]);
+        }
+#pragma unroll
+        for (int u = 0; u < TA3B_ILP; ++u) {
+            uint64_t key = 0;
+            bool const def = valid[u] && st[u] != FAST_OK;
+            if (valid[u] && st[u] == FAST_OK) {
+                key = candidate_key(leaf, v[u], info[u], idx[u]);
+                consume(key, sg[u], info[u]);
+            }
+            uint32_t const dm = __ballot_sync(FULL_MASK, def);
+            if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = (sg[u] << 8) | idx[u];
+            queued += __popc(dm);
+            fold(key);
+            if (queued >= uint32_t(WARP)) {
+                __syncwarp();
+                drain(WARP, queued);
+                queued -= WARP;
+            }
         }
     }
     __syncwarp();
@@ -845,47 +720,19 @@ __device__ __noinline__ void root_record(WarpShared* ws, int lane) {
     __syncwarp();
 }
 
-extern __shared__ __align__(16) unsigned char dyn_smem[];        // the block's WarpShared areas (then hb)
-__device__ __forceinline__ WarpShared* block_ws() { return reinterpret_cast<WarpShared*>(dyn_smem); }
-
-// owner, after a stage's second barrier: fold the helpers' results into its own
-__device__ __forceinline__ void team_merge(WarpShared& ws, uint32_t size, LevelAcc& a, bool leaf, int kl, int lane,
-                                           uint32_t& evals) {
-    for (uint32_t k = 1; k < size; ++k) {
-        uint64_t const* x = reinterpret_cast<uint64_t const*>(block_ws()[ws.team.member[k - 1]].rec);
-        if (!leaf) a.list = merge_topk(a.list, x[lane], kl, lane);
-        if (lane == 0) {
-            if (leaf) a.best = x[X_BEST] > a.best ? x[X_BEST] : a.best;
-            uint64_t const bits = x[X_BITS];
-            a.lo |= uint32_t(bits);
-            a.hi |= uint32_t(bits >> 32);
-            evals += uint32_t(x[X_EVALS]);
-        }
-    }
-}
-
-// search_move_beam (beam.hpp:484-570) for one move of game g. self is the calling
-// warp's own area (its deferred-candidate queue, a helper's exchange words).
-// The owner (help = false, g == self) plays the move; with a team (TEAM kernels,
-// g.team.size > 1) it publishes each stage, takes its share of the candidates and
-// merges the helpers' results. A helper (help = true, member `index` of g's team)
-// follows the owner's published stages, taking its share of each, until the game
-// ends; it returns (with mv.none) only then. Both roles run the one inlined copy
-// of level_pass, so the kernel holds a single copy of the candidate loop.
-template <int NET, bool KEYS, bool TEAM>
-__device__ __forceinline__ Move search_move(WarpShared& g, WarpShared& self, bool help, uint32_t index, Luts lut,
-                                            FastW const& fw, float* hb, int lane, uint32_t& evals, uint32_t* status) {
+// search_move_beam (beam.hpp:484-570) for the warp's committed game
+template <int NET, bool KEYS>
+__device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
+                                            uint32_t* status) {
     constexpr bool WIDE = NET != 0;
-    help = TEAM && help;
-    uint32_t const first = help ? index * uint32_t(WARP) : 0u;   // this warp's first round of a stage
     Move mv{0, 0, 0, true, 0, 0};
-    if (!help && g.eng.over) return mv;
+    if (ws.eng.over) return mv;
     uint32_t slot_piece[NSLOTS];                                  // beam.hpp:226-237
-    slot_piece[0] = g.eng.held;
-    slot_piece[1] = g.eng.queue[0];
+    slot_piece[0] = ws.eng.held;
+    slot_piece[1] = ws.eng.queue[0];
 #pragma unroll
-    for (int i = 0; i < DEPTH; ++i) slot_piece[2 + i] = g.eng.queue[1 + i];
-    int const tree = g.eng.held == NO_PIECE ? 1 : 0;
+    for (int i = 0; i < DEPTH; ++i) slot_piece[2 + i] = ws.eng.queue[1 + i];
+    int const tree = ws.eng.held == NO_PIECE ? 1 : 0;
     uint32_t const r0 = c_tables.node[tree][0][0], r1 = c_tables.node[tree][0][1];
     uint32_t const p0 = slot_piece[r0 & 0xFu], p1 = slot_piece[r1 & 0xFu];
 
@@ -894,84 +741,41 @@ __device__ __forceinline__ Move search_move(WarpShared& g, WarpShared& self, boo
     uint64_t best = 0;                         // leaf-order (score | order) maximum, fallbacks included
     uint64_t best2 = 0;                        // the second-largest such key (tracing flavour)
 #pragma unroll 1
-    for (int stage = 0; help || stage < DEPTH;) {
-        uint32_t total, tsize;
-        if (help) {
-            // ---- the owner's next stage, or the end of its game
-            if (!team_sync_member(&g.team, status, lane)) return mv;
-            uint32_t const cmd = *reinterpret_cast<volatile uint32_t*>(&g.team.cmd);
-            if (cmd == CMD_RELEASE) return mv;
-            stage = int(cmd);
-            total = *reinterpret_cast<volatile uint32_t*>(&g.team.total);
-            tsize = *reinterpret_cast<volatile uint32_t*>(&g.team.size);
-        } else {
-            // ---- segments of this stage
-            if (stage == 0) {                  // two root groups over the committed board (beam.hpp:283-301)
-                root_record<WIDE>(&g, lane);
-                if (lane < 2) {
-                    uint32_t const nd = lane ? r1 : r0;
-                    uint32_t const held_slot = (nd >> 4) & 0xFu;
-                    uint32_t const held_i = held_slot != HELD_NONE && slot_piece[held_slot] == 0u;
-                    g.seg_info[lane] = 32u | ((lane ? p1 : p0) << 16) | (held_i << 20) | (uint32_t(lane) << 21);
-                }
-                total = c_tables.nplace[p0] + c_tables.nplace[p1];
-                if (lane == 0) {
-                    g.seg_off[0] = 0;
-                    g.seg_off[1] = c_tables.nplace[p0];
-                    g.seg_off[2] = total;
-                    g.seg_off[3] = total;
-                }
-                __syncwarp();
-            } else {
-                total = build_segments(g, slot_piece, tree, stage, fnode, kept, lane);
-            }
-            // ---- with helpers, the stage goes out to the team
-            tsize = TEAM && !g.team.broken ? g.team.size : 1u;
-            if (TEAM && tsize > 1) {
-                if (lane == 0) {
-                    g.team.cmd = uint32_t(stage);
-                    g.team.total = total;
-                }
-                if (!team_sync_owner(&g.team, tsize, status, lane)) g.team.broken = 1;
-            }
-        }
+    for (int stage = 0; stage < DEPTH; ++stage) {
         bool const leaf = stage == DEPTH - 1;
-        int const kl = stage == 0 ? K0 : (stage == 1 ? K1 : K2);
-        // ---- every candidate of the stage (this warp's rounds of it, in a team)
-        uint32_t lev = 0;
-        LevelAcc a = level_pass<NET, KEYS>(g, self.defer, lut, fw, hb, leaf, total, kl, lane, lev, first,
-                                           tsize * uint32_t(WARP));
-        if (help) {
-            // ---- leave this warp's part for the owner (in its own, unused record area)
-            uint64_t* const x = reinterpret_cast<uint64_t*>(self.rec);
-            uint64_t const bw = warp_max64(a.best);
-            uint32_t const lo = __reduce_or_sync(FULL_MASK, a.lo), hi = __reduce_or_sync(FULL_MASK, a.hi);
-            uint32_t const ev = __reduce_add_sync(FULL_MASK, lev);
-            if (!leaf) x[lane] = a.list;
-            if (lane == 0) {
-                x[X_BEST] = bw;
-                x[X_BITS] = uint64_t(lo) | (uint64_t(hi) << 32);
-                x[X_EVALS] = ev;
+        // ---- segments of this stage
+        uint32_t total;
+        if (stage == 0) {                      // two root groups over the committed board (beam.hpp:283-301)
+            root_record<WIDE>(&ws, lane);
+            if (lane < 2) {
+                uint32_t const nd = lane ? r1 : r0;
+                uint32_t const held_slot = (nd >> 4) & 0xFu;
+                uint32_t const held_i = held_slot != HELD_NONE && slot_piece[held_slot] == 0u;
+                ws.seg_info[lane] = 32u | ((lane ? p1 : p0) << 16) | (held_i << 20) | (uint32_t(lane) << 21);
             }
-            if (!team_sync_member(&g.team, status, lane)) return mv;
-            continue;
+            total = c_tables.nplace[p0] + c_tables.nplace[p1];
+            if (lane == 0) {
+                ws.seg_off[0] = 0;
+                ws.seg_off[1] = c_tables.nplace[p0];
+                ws.seg_off[2] = total;
+                ws.seg_off[3] = total;
+            }
+            __syncwarp();
+        } else {
+            total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
-        evals += lev;
-        if (TEAM && !g.team.broken && g.team.size > 1) {
-            if (team_sync_owner(&g.team, g.team.size, status, lane))
-                team_merge(g, g.team.size, a, leaf, kl, lane, evals);   // the helpers' results in
-            else
-                g.team.broken = 1;
-        }
+        // ---- every candidate of the stage
+        LevelAcc const a = level_pass<NET, KEYS>(ws, lut, fw, hb, leaf, total,
+                                                   stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane, evals);
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
             kept = __popc(__ballot_sync(FULL_MASK, a.list != 0));
             if (kept == 0) return mv;                             // no legal root: game over
             root_slot = 0xFFFFFFFFu - uint32_t(a.list);
             fscore = uint32_t(a.list >> 32);
-            uint32_t const grp = lane < kept ? root_slot / MP : 0u;
-            fnode = grp;
-            materialize<WIDE>(&g, lut, lane < kept, 32u, grp ? p1 : p0, root_slot % MP, lane);
+            uint32_t const g = lane < kept ? root_slot / MP : 0u;
+            fnode = g;
+            materialize<WIDE>(&ws, lut, lane < kept, 32u, g ? p1 : p0, root_slot % MP, lane);
         } else if (!leaf) {
             uint32_t const has_child = __reduce_or_sync(FULL_MASK, a.lo);
             // kept nodes with no legal continuation become leaves at this depth (beam.hpp:549-551)
@@ -989,7 +793,7 @@ __device__ __forceinline__ Move search_move(WarpShared& g, WarpShared& self, boo
             uint32_t const par_rank = __shfl_sync(FULL_MASK, frank, int(pk));
             uint32_t const cnode = (2u * par_node + child) & 15u;
             uint32_t const piece = slot_piece[c_tables.node[tree][stage][cnode] & 0xFu];
-            materialize<WIDE>(&g, lut, lane < next, pk, piece, sslot % MP, lane);
+            materialize<WIDE>(&ws, lut, lane < next, pk, piece, sslot % MP, lane);
             fscore = uint32_t(a.list >> 32);
             fnode = lane < next ? cnode : 0u;
             frank = par_rank;
@@ -1017,7 +821,6 @@ __device__ __forceinline__ Move search_move(WarpShared& g, WarpShared& self, boo
                 }
             }
         }
-        ++stage;
     }
     if (KEYS) {
         warp_top2(best, best2);
@@ -1035,75 +838,13 @@ __device__ __forceinline__ Move search_move(WarpShared& g, WarpShared& self, boo
     uint32_t const leaf_rank = __shfl_sync(FULL_MASK, frank, int((order / (2 * MP)) & 31u));
     uint32_t const rank = order >= uint32_t(LEAF_ORDERS) ? order - LEAF_ORDERS : leaf_rank;
     uint32_t const rs = __shfl_sync(FULL_MASK, root_slot, int(rank & 31u));
-    uint32_t const grp = rs / MP;
-    uint32_t const pa = lut.move[grp ? p1 : p0][rs % MP];
+    uint32_t const g = rs / MP;
+    uint32_t const pa = lut.move[g ? p1 : p0][rs % MP];
     mv.orient = int((pa >> 20) & 3u);
     mv.x = int((pa >> 24) & 0xFu) - 2;
-    mv.hold = int((c_tables.node[tree][0][grp] >> 8) & 1u);
+    mv.hold = int((c_tables.node[tree][0][g] >> 8) & 1u);
     mv.none = ordered_bits_inv(uint32_t(best >> 32)) == -__int_as_float(0x7f800000);   // search.hpp:41
     return mv;
-}
-
-// A warp with no sim left asks to join a game of its block: the open team with the fewest
-// join requests. Returns the owner's warp and its member index, or -1 when no game of the
-// block is open (or a wait ran out).
-__device__ __forceinline__ int team_request(WarpShared* blk, int nwarps, int me, uint32_t& index, uint32_t* status,
-                                           int lane) {
-    for (;;) {
-        uint32_t key = 0xFFFFFFFFu;
-        if (lane < nwarps && lane != me) {
-            TeamState* const t = &blk[lane].team;
-            if (*reinterpret_cast<volatile uint32_t*>(&t->state) == TEAM_OPEN) {
-                uint32_t const q = *reinterpret_cast<volatile uint32_t*>(&t->req);
-                if (q < kMaxTeam - 1) key = (q << 5) | uint32_t(lane);
-            }
-        }
-        key = __reduce_min_sync(FULL_MASK, key);
-        if (key == 0xFFFFFFFFu) return -1;
-        int const owner = int(key & 31u);
-        int res = -1;                                            // 1 joined, 0 look again, -1 give up
-        uint32_t idx = 0;
-        if (lane == 0) {
-            TeamState* const t = &blk[owner].team;
-            uint32_t const r = atomicAdd(&t->req, 1u);
-            if (r >= kMaxTeam - 1) {
-                res = 0;                                         // the team filled up meanwhile
-            } else {
-                uint32_t const mine = uint32_t(me) + 1u;
-                atomicExch(&t->join[r], mine);                   // post the request
-                unsigned long long const t0 = global_ns();
-                for (;;) {
-                    uint32_t const v = *reinterpret_cast<volatile uint32_t*>(&t->join[r]);
-                    if (v & JOIN_ADMIT) {
-                        res = 1;
-                        idx = v >> 16;
-                        break;
-                    }
-                    bool const closed = *reinterpret_cast<volatile uint32_t*>(&t->state) != TEAM_OPEN;
-                    bool const late = global_ns() - t0 > kTeamWaitNs;
-                    if (closed || late) {                        // withdraw, unless admitted meanwhile
-                        uint32_t const got = atomicCAS(&t->join[r], mine, mine | JOIN_WITHDRAWN);
-                        if (got == mine) {
-                            res = late ? -1 : 0;
-                            if (late) atomicOr(status, STATUS_TEAM);
-                        } else {
-                            res = 1;
-                            idx = got >> 16;
-                        }
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-            __threadfence_block();
-        }
-        res = __shfl_sync(FULL_MASK, res, 0);
-        if (res == 1) {
-            index = __shfl_sync(FULL_MASK, idx, 0);
-            return owner;
-        }
-        if (res < 0) return -1;
-    }
 }
 
 // NET: 0 = the v11 model; H = the widened 10 -> H -> H -> 1 network (64: 4,929 weights per
@@ -1115,87 +856,56 @@ template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = fal
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;
-    // warps with no sim left join games of their block (the v11 kernels; the budget and
-    // key-tracing flavours and the widened networks play every game alone)
-    constexpr bool TEAM = NET == 0 && !BUDGET && !KEYS && WARPS > 1 && WARPS <= int(kMaxTeam);
+    extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
-    int const lane = int(threadIdx.x & 31u);
-    int const warp = int(threadIdx.x >> 5);
-    WarpShared* const blk = block_ws();
-    WarpShared& ws = blk[warp];
-    uint32_t* const status = &p.scratch[kStatusWord];
     for (int t = int(threadIdx.x); t < NPIECE * MP; t += WARPS * 32) {
         s_lut.fast[t / MP][t % MP] = g_lut.fast[t / MP][t % MP];
         s_lut.move[t / MP][t % MP] = g_lut.move[t / MP][t % MP];
     }
-    if (TEAM && lane == 0) ws.team.state = TEAM_CLOSED;         // before any warp of the block looks
     __syncthreads();
     Luts const lut{s_lut.fast, s_lut.move};
+    int const lane = int(threadIdx.x & 31u);
+    WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
     // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
     float* const hb = WIDE ? reinterpret_cast<float*>(dyn_smem + WARPS * sizeof(WarpShared)) +
                                  (threadIdx.x >> 5) * kWideHbFloats<HW>
                            : nullptr;
     // time budget, measured from this warp's start (the persistent grid starts every warp at launch);
     // kept in shared memory so it costs no register in the move loop
-    if (BUDGET && lane == 0) ws.t_start = global_ns();
-    FastW fw;                                  // the fast path's weights of the game being played
-    bool drained = false;                      // the work queue is empty (TEAM: this warp only helps now)
+    if (BUDGET && lane == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(ws.t_start));
     for (;;) {
-        // ---- the next game: a sim of this warp's own, or (queue empty) a game of the block to help
-        uint32_t sim = kNoSim;
-        if (!drained) {
-            // a 64-bit ticket: every resident warp draws one past the last sim, which a 32-bit
-            // counter could wrap near 2^32 sims; kNoSim (no sim index is that large) means empty
-            if (lane == 0) {
-                unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
-                sim = t < p.total_sims ? uint32_t(t) : kNoSim;
-            }
-            sim = __shfl_sync(FULL_MASK, sim, 0);
-            drained = sim == kNoSim;
+        // a 64-bit ticket: every resident warp draws one past the last sim, which a 32-bit
+        // counter could wrap near 2^32 sims; kNoSim (no sim index is that large) ends the warp
+        uint32_t sim = 0;
+        if (lane == 0) {
+            unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
+            sim = t < p.total_sims ? uint32_t(t) : kNoSim;
         }
-        bool const help = TEAM && drained;
-        uint32_t index = 0;
-        WarpShared* gp = &ws;
-        if (drained) {
-            if (!TEAM) break;
-            int const owner = team_request(blk, WARPS, warp, index, status, lane);
-            if (owner < 0) break;
-            gp = &blk[owner];
-            if (!WIDE) load_fast_weights(SmemW{gp->wfull}, fw);
-        } else {
-            uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
-            uint32_t const island = mdl / p.models_per_island;
-            uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
-            float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WideNet<HW>::STRIDE : NPARAMS);
-            if (p.timing && lane == 0) p.timing[2 * size_t(sim)] = global_ns();
-            if (!WIDE) {
-                load_fast_weights(GlobalW{wsrc}, fw);
-                for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
-            }
-            if (lane == 0) {
-                ws.wglobal = wsrc;
-                engine_reset(ws.eng, seed);
-                ws.st = Stats{};
-                if (TEAM) {                                      // a new game takes no helpers yet
-                    ws.team.req = 0;
-                    ws.team.scan = 0;
-                    ws.team.size = 1;
-                    ws.team.count = 0;
-                    ws.team.cmd = 0;
-                    ws.team.broken = 0;
-                    for (uint32_t k = 0; k + 1 < kMaxTeam; ++k) ws.team.join[k] = 0;
-                    __threadfence_block();
-                    *reinterpret_cast<volatile uint32_t*>(&ws.team.state) = TEAM_OPEN;
-                }
-            }
-            __syncwarp();
+        sim = __shfl_sync(FULL_MASK, sim, 0);
+        if (sim == kNoSim) break;
+        uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
+        uint32_t const island = mdl / p.models_per_island;
+        uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
+        float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WideNet<HW>::STRIDE : NPARAMS);
+        if (p.timing && lane == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            p.timing[2 * size_t(sim)] = t;
         }
-        // ---- play it (a helper's search_move returns at the end of the owner's game)
+        FastW fw;
+        if (!WIDE) {
+            load_fast_weights(GlobalW{wsrc}, fw);
+            for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
+        }
+        if (lane == 0) {
+            ws.wglobal = wsrc;
+            engine_reset(ws.eng, seed);
+            ws.st = Stats{};
+        }
+        __syncwarp();
         uint32_t evals = 0, moves = 0;
-        for (uint32_t mv_i = 0; help || (mv_i < p.max_moves && !ws.eng.over); ++mv_i) {   // model_eval_host.cpp:39-50
-            if (TEAM && !help) team_admit(&ws.team, lane);      // helpers join between moves
-            Move const mv = search_move<NET, KEYS, TEAM>(*gp, ws, help, index, lut, fw, hb, lane, evals, status);
-            if (help || (TEAM && ws.team.broken)) break;         // helped to the end / a team wait ran out
+        for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
+            Move const mv = search_move<NET, KEYS>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
             if (KEYS && lane == 0 && p.keys) {
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2] = mv.key1;
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2 + 1] = mv.key2;
@@ -1217,24 +927,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             __syncwarp();
             if (ws.eng.over == 2) break;
             if (BUDGET) {                                          // over = 3: out of time, stop here
-                if (lane == 0 && global_ns() - ws.t_start > p.budget_ns) {
-                    atomicOr(status, 2u);
-                    ws.eng.over = 3;
+                if (lane == 0) {
+                    unsigned long long now;
+                    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+                    if (now - ws.t_start > p.budget_ns) {
+                        atomicOr(&p.scratch[kStatusWord], 2u);
+                        ws.eng.over = 3;
+                    }
                 }
                 __syncwarp();
                 if (ws.eng.over == 3) break;
             }
-        }
-        if (help) continue;
-        if (TEAM) {                                              // no more helpers; release the team
-            uint32_t const tsize = ws.team.size;
-            if (lane == 0) {
-                *reinterpret_cast<volatile uint32_t*>(&ws.team.state) = TEAM_CLOSED;
-                if (tsize > 1) ws.team.cmd = CMD_RELEASE;
-                __threadfence_block();
-            }
-            __syncwarp();
-            if (tsize > 1) team_sync_owner(&ws.team, tsize, status, lane);
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
         if (lane == 0) {
@@ -1245,7 +948,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             if (p.n_moves) p.n_moves[sim] = moves;
             if (p.board_out)
                 for (int x = 0; x < W; ++x) p.board_out[size_t(sim) * W + x] = ws.eng.board[x];
-            if (p.timing) p.timing[2 * size_t(sim) + 1] = global_ns();
+            if (p.timing) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                p.timing[2 * size_t(sim) + 1] = t;
+            }
         }
         __syncwarp();
         if (BUDGET && ws.eng.over == 3) break;                   // out of time: take no further sim
@@ -1265,7 +972,8 @@ __global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand,
     FastW fw;
     load_fast_weights(GlobalW{w}, fw);
     float v = 0.0f;
-    // the kernel's own arithmetic mode, then (diagnostics) the other two: all must agree bit for bit
+    // the kernel's own arithmetic mode, then (diagnostics) every MLP mode: scalar, packed
+    // intrinsics, packed PTX
     fast_st[t] = fast_candidate(rec, g_lut.fast[piece][i], held, fw, v, dbg ? dbg + size_t(t) * 32 : nullptr);
     if (dbg) {
         float v2 = 0.0f, v3 = 0.0f, v4 = 0.0f;
