@@ -59,9 +59,9 @@ METRIC_WIDE32 = ("beam placements/s on 1 B200 (widened 10-32-32-1 evaluator: 8 i
 METRICS = {"wide": METRIC_WIDE, "wide32": METRIC_WIDE32, "stress": METRIC_STRESS}
 HIDDEN = {"wide": 64, "wide32": 32}           # the widened models' hidden width
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
-# on the small-case capture) and its DRAM bytes per full-generation launch
+# on the full-occupancy capture, profiles/eval_kernel_full_occupancy.md) and its DRAM bytes per full-generation launch
 # (ncu dram__bytes_read.sum + dram__bytes_write.sum, 1-pass capture of the full launch).
-LANE_INSTR_PER_PLACEMENT = 564
+LANE_INSTR_PER_PLACEMENT = 592
 DRAM_BYTES_PER_LAUNCH = 888_576
 
 
