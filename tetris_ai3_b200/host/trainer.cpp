@@ -120,7 +120,7 @@ struct GpuSurrogate {
     ta3s_model* model = nullptr;
     ta3w_model* wide = nullptr;
     uint32_t epochs = 40, batch = 256, trainings = 0;
-    float lr = 1e-3f, weight_decay = 1e-2f;
+    float lr = 1e-3f, weight_decay = 0.0f;      // plain Adam (the kernels also take a decoupled decay)
     ~GpuSurrogate() {
         if (model) ta3s_destroy(model);
         if (wide) ta3w_destroy(wide);

@@ -63,7 +63,7 @@ class Surrogate:
     without an sm_100 device."""
 
     def __init__(self, device: int = 0, seed: int = 0, epochs: int = 40, batch: int = 256, lr: float = 1e-3,
-                 weight_decay: float = 1e-2, in_dim: int = 97, hidden: int = 128):
+                 weight_decay: float = 0.0, in_dim: int = 97, hidden: int = 128):
         self.lib = _lib()
         self.in_dim, self.hidden = in_dim, hidden
         self.fused = (in_dim, hidden) == V11_SHAPE
