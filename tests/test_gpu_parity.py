@@ -228,10 +228,11 @@ def test_device_core_matches_host_core(ev):
     # separately rounded operations once compiled, see the kernel's MLP mode notes)
     ok = fs == 0
     bad = {name: int((ok & (dd[:, slot].view(np.uint32) != fv.view(np.uint32))).sum())
-           for name, slot in (("scalar", 29), ("packed intrinsics", 30), ("packed PTX", 31))}
+           for name, slot in (("packed multiplies", 28), ("scalar", 29), ("packed intrinsics", 30),
+                              ("packed PTX", 31))}
     print("MLP mode mismatches:", bad, "of", int(ok.sum()))
     assert not mism, f"{len(mism)} of {n} candidates differ"
-    assert bad["scalar"] == 0, bad
+    assert bad["scalar"] == 0 and bad["packed multiplies"] == 0, bad
 
 
 def test_generation_graph_replays_match_direct_calls(ev):

@@ -689,13 +689,20 @@ __device__ __forceinline__ uint32_t build_segments(WarpShared& ws, uint32_t cons
     return base;
 }
 
-// lane j builds kept node j (when active): parent record `prec`, placement (piece, i)
+#ifndef TA3B_ONE_BUILDER
+#define TA3B_ONE_BUILDER 0
+#endif
+
+// lane j builds kept node j (when active): parent record `prec`, placement (piece, i); with
+// root, the active lane builds record 32 from the committed board (no placement, no clears)
 template <bool WIDE>
 __device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, uint32_t prec, uint32_t piece,
-                                         uint32_t i, int lane) {
+                                         uint32_t i, int lane, bool root = false) {
     uint32_t nb[W];
     uint32_t ncl = 0;
-    if (active) {
+    if (active && root) {
+        load_board(ws->eng.board, nb);
+    } else if (active) {
         uint32_t const* pr = ws->rec[prec];
         uint32_t b[W];
         load_board(pr + R_BOARD, b);
@@ -705,19 +712,23 @@ __device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, 
         ncl = pr[R_CLEARS] + clear_bump(cl);
     }
     __syncwarp();
-    if (active) build_record<SmemW, !WIDE>(nb, ncl, SmemW{ws->wfull}, ws->rec[lane]);
+    if (active) build_record<SmemW, !WIDE>(nb, ncl, SmemW{ws->wfull}, ws->rec[root ? 32 : lane]);
     __syncwarp();
 }
 
 // the committed board's record (record 32): one lane builds it, the warp waits
 template <bool WIDE>
-__device__ __noinline__ void root_record(WarpShared* ws, int lane) {
+__device__ __noinline__ void root_record(WarpShared* ws, Luts lut, int lane) {
+#if TA3B_ONE_BUILDER
+    materialize<WIDE>(ws, lut, lane == 0, 0u, 0u, 0u, lane, true);       // the same record-builder body
+#else
     if (lane == 0) {
         uint32_t b[W];
         load_board(ws->eng.board, b);
         build_record<SmemW, !WIDE>(b, 0u, SmemW{ws->wfull}, ws->rec[32]);
     }
     __syncwarp();
+#endif
 }
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
@@ -746,7 +757,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         // ---- segments of this stage
         uint32_t total;
         if (stage == 0) {                      // two root groups over the committed board (beam.hpp:283-301)
-            root_record<WIDE>(&ws, lane);
+            root_record<WIDE>(&ws, lut, lane);
             if (lane < 2) {
                 uint32_t const nd = lane ? r1 : r0;
                 uint32_t const held_slot = (nd >> 4) & 0xFu;
@@ -976,10 +987,12 @@ __global__ void core_selftest_kernel(uint32_t const* recs, uint32_t const* cand,
     // intrinsics, packed PTX
     fast_st[t] = fast_candidate(rec, g_lut.fast[piece][i], held, fw, v, dbg ? dbg + size_t(t) * 32 : nullptr);
     if (dbg) {
-        float v2 = 0.0f, v3 = 0.0f, v4 = 0.0f;
+        float v2 = 0.0f, v3 = 0.0f, v4 = 0.0f, v5 = 0.0f;
         fast_candidate<MLP_PTX_X2>(rec, g_lut.fast[piece][i], held, fw, v2, nullptr);
         fast_candidate<MLP_X2>(rec, g_lut.fast[piece][i], held, fw, v3, nullptr);
         fast_candidate<MLP_SCALAR>(rec, g_lut.fast[piece][i], held, fw, v4, nullptr);
+        fast_candidate<MLP_X2MUL>(rec, g_lut.fast[piece][i], held, fw, v5, nullptr);
+        dbg[size_t(t) * 32 + 28] = v5;
         dbg[size_t(t) * 32 + 29] = v4;
         dbg[size_t(t) * 32 + 30] = v3;
         dbg[size_t(t) * 32 + 31] = v2;
