@@ -186,20 +186,41 @@ __device__ void engine_hold(Engine& e) {                                     // 
     update_game_over(e);
 }
 
-// hard drop at window x-origin x in orientation o; returns rows cleared or -1 on top-out
-__device__ int engine_place(Engine& e, int o, int x) {                       // tetris_engine.hpp:137-146
+__device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uint32_t (&b)[W]);
+
+// The drop + lock + clear of one placement (search.hpp:61-70, board2.hpp:306-342) and the
+// integer metrics of the resulting board (v_board_metrics.hpp:130-225): one body for the
+// deferred candidates' full path and the engine's commit, so the kernel holds one copy of
+// it. src is 16-byte aligned; dst (may be null, may equal src) receives the new board.
+struct Applied {
+    BoardInts bi;
+    int cleared;
+    bool legal;
+};
+__device__ __noinline__ Applied apply_ints(uint32_t const* src, uint32_t cols, int col0, uint32_t* dst) {
+    uint32_t b[W], nb[W];
+    load_board(src, b);
+    Applied r{};
+    r.legal = apply_full(b, cols, col0, nb, r.cleared);
+    if (!r.legal) return r;
+    r.bi = board_ints(nb);
+    if (dst)
+        for (int c = 0; c < W; ++c) dst[c] = nb[c];
+    return r;
+}
+
+// hard drop at window x-origin x in orientation o; returns rows cleared or -1 on top-out,
+// and the new board's metrics in bi
+__device__ int engine_place(Engine& e, int o, int x, BoardInts& bi) {         // tetris_engine.hpp:137-146
     uint32_t const p = e.queue[0];
     uint32_t const cols = c_tables.shape_cols[p][o];
     int const col0 = x + c_tables.shape_left[p][o];
-    uint32_t b[W], nb[W];
-    for (int c = 0; c < W; ++c) b[c] = e.board[c];
-    int cleared = 0;
     // the search only commits legal moves, so this is the drop + lock + clear of board2.hpp
-    apply_full(b, cols, col0, nb, cleared);
-    for (int c = 0; c < W; ++c) e.board[c] = nb[c];
+    Applied const a = apply_ints(e.board, cols, col0, e.board);
+    bi = a.bi;
     advance_queue(e);
     update_game_over(e);
-    return e.over ? -1 : cleared;
+    return e.over ? -1 : a.cleared;
 }
 
 // ------------------------------------------------------------ candidates ---
@@ -222,11 +243,8 @@ __device__ __forceinline__ void load_board(uint32_t const* __restrict__ src, uin
     b[8] = q2.x; b[9] = q2.y;
 }
 
-#ifndef TA3B_ILP
-#define TA3B_ILP 1
-#endif
 #ifndef TA3B_MLP_MODE
-#define TA3B_MLP_MODE MLP_SCALAR
+#define TA3B_MLP_MODE MLP_X2MUL     // packed multiplies, scalar adds: the reference's roundings, fewer instructions
 #endif
 
 // fast path: read the parent-record words this placement needs, then eval_core's fast_eval
@@ -364,11 +382,8 @@ __device__ __forceinline__ int fast_candidate_wide(uint32_t const* __restrict__ 
     return defer ? FAST_DEFER : FAST_OK;
 }
 
-// stats_v4::advance (tetris_stats.hpp:19-23 with metrics.hpp:196-229)
-__device__ void stats_advance(Stats& st, uint32_t const* board, uint32_t lines) {
-    uint32_t b[W];
-    for (int x = 0; x < W; ++x) b[x] = board[x];
-    BoardInts const bi = board_ints(b);
+// stats_v4::advance (tetris_stats.hpp:19-23 with metrics.hpp:196-229); bi: the board's metrics
+__device__ void stats_advance(Stats& st, BoardInts const& bi, uint32_t lines) {
     st.pieces += 1;
     st.lines += lines;
     st.clears[lines] += 1;
@@ -515,12 +530,9 @@ __device__ __noinline__ uint64_t full_key(WarpShared* ws, Luts lut, bool leaf, u
     uint32_t const info = ws->seg_info[seg];
     uint32_t const* rec = ws->rec[info & 63u];
     uint32_t const mv = lut.move[(info >> 16) & 7u][i];
-    uint32_t b[W], nb[W];
-    load_board(rec + R_BOARD, b);
-    int cl = 0;
-    if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return 0;
-    BoardInts const bi = board_ints(nb);
-    float const v = value_full(rec[R_CLEARS] + clear_bump(cl), bi, (info >> 20) & 1u, SmemW{ws->wfull});
+    Applied const a = apply_ints(rec + R_BOARD, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nullptr);
+    if (!a.legal) return 0;
+    float const v = value_full(rec[R_CLEARS] + clear_bump(a.cleared), a.bi, (info >> 20) & 1u, SmemW{ws->wfull});
     return candidate_key(leaf, v, info, i);
 }
 
@@ -531,11 +543,9 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
     uint32_t const info = ws->seg_info[seg];
     uint32_t const* rec = ws->rec[info & 63u];
     uint32_t const mv = lut.move[(info >> 16) & 7u][i];
-    uint32_t b[W], nb[W];
-    load_board(rec + R_BOARD, b);
-    int cl = 0;
-    if (!apply_full(b, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nb, cl)) return false;
-    wide_inputs(rec[R_CLEARS] + clear_bump(cl), board_ints(nb), (info >> 20) & 1u, in.v);
+    Applied const a = apply_ints(rec + R_BOARD, mv & 0xFFFFu, int((mv >> 16) & 0xFu), nullptr);
+    if (!a.legal) return false;
+    wide_inputs(rec[R_CLEARS] + clear_bump(a.cleared), a.bi, (info >> 20) & 1u, in.v);
     return true;
 }
 
@@ -557,102 +567,85 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
             else acc.hi |= 1u << (bit - 32);
         }
     };
-    auto fold = [&](uint64_t key) {
+    // Each iteration is one round of 32 fast-path candidates (one per lane) or, once 32 are
+    // queued (or the level is done), one batch of up to 32 deferred candidates through the full
+    // path; either way its keys are folded at one place. Keys are unique within a level, so the
+    // fold order does not change the kept set. One drain site and one fold site keep the loop's
+    // code small (the kernel is bound by instruction fetch as much as by issue). Two candidates
+    // per lane in straight-line code measured slower (681 ms vs 486 ms per full generation).
+    uint32_t queued = 0;          // < 32 at the start of every fast round: the queue holds 64
+    int seg = 0;
+    uint32_t c0 = 0;
+    for (;;) {
+        bool const more = c0 < total;
+        if (!more && queued == 0) break;
+        uint64_t key = 0;
+        if (queued >= uint32_t(WARP) || !more) {
+            // ---- a batch of deferred candidates through the full reference path
+            uint32_t const n = queued < uint32_t(WARP) ? queued : uint32_t(WARP);
+            __syncwarp();
+            if constexpr (WIDE) {
+                // the inputs per lane, then the network on all lanes together
+                WideIn in{};
+                uint32_t entry = 0;
+                bool legal = false;
+                if (uint32_t(lane) < n) {
+                    entry = ws.defer[lane];
+                    legal = full_inputs_wide(&ws, lut, entry, in);
+                    if (!legal) in = WideIn{};
+                }
+                __syncwarp();
+                float const v = wide_value<HW>(in, ws.wglobal, hb, lane);
+                if (legal) {
+                    uint32_t const info = ws.seg_info[entry >> 8];
+                    key = candidate_key(leaf, v, info, entry & 0xFFu);
+                    consume(key, entry >> 8, info);
+                }
+            } else if (uint32_t(lane) < n) {
+                uint32_t const entry = ws.defer[lane];
+                key = full_key(&ws, lut, leaf, entry);
+                consume(key, entry >> 8, ws.seg_info[entry >> 8]);
+            }
+            uint32_t const rem = queued - n;
+            uint32_t t = 0;
+            __syncwarp();
+            if (uint32_t(lane) < rem) t = ws.defer[n + lane];
+            __syncwarp();
+            if (uint32_t(lane) < rem) ws.defer[lane] = t;
+            __syncwarp();
+            queued = rem;
+        } else {
+            // ---- a round of fast-path candidates
+            uint32_t const c = c0 + uint32_t(lane);
+            bool const valid = c < total;
+            uint32_t const cc = valid ? c : total - 1u;          // out of range: the last candidate, discarded
+            while (ws.seg_off[seg + 1] <= cc) ++seg;
+            uint32_t const sg = uint32_t(seg);
+            uint32_t const info = ws.seg_info[seg];
+            uint32_t const idx = cc - ws.seg_off[seg];
+            float v;
+            int st;
+            if constexpr (WIDE)
+                st = fast_candidate_wide<HW>(ws.rec[info & 63u], lut.fast[(info >> 16) & 7u][idx], (info >> 20) & 1u,
+                                             ws.wglobal, hb, lane, v);
+            else
+                st = fast_candidate(ws.rec[info & 63u], lut.fast[(info >> 16) & 7u][idx], (info >> 20) & 1u, fw, v);
+            bool const def = valid && st != FAST_OK;
+            if (valid && st == FAST_OK) {
+                key = candidate_key(leaf, v, info, idx);
+                consume(key, sg, info);
+            }
+            uint32_t const dm = __ballot_sync(FULL_MASK, def);
+            if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = (sg << 8) | idx;
+            queued += __popc(dm);
+            c0 += WARP;
+        }
         if (leaf) {
             if (KEYS) top2_insert(acc.best, acc.best2, key);
             else acc.best = key > acc.best ? key : acc.best;
         } else {
             topk_fold(acc.list, acc.thr, key, kl, lane);
         }
-    };
-    auto drain = [&](uint32_t n, uint32_t queued) {
-        uint64_t key = 0;
-        if constexpr (WIDE) {
-            // the inputs per lane, then the network on all lanes together
-            WideIn in{};
-            uint32_t entry = 0;
-            bool legal = false;
-            if (uint32_t(lane) < n) {
-                entry = ws.defer[lane];
-                legal = full_inputs_wide(&ws, lut, entry, in);
-                if (!legal) in = WideIn{};
-            }
-            __syncwarp();
-            float const v = wide_value<HW>(in, ws.wglobal, hb, lane);
-            if (legal) {
-                uint32_t const info = ws.seg_info[entry >> 8];
-                key = candidate_key(leaf, v, info, entry & 0xFFu);
-                consume(key, entry >> 8, info);
-            }
-        } else if (uint32_t(lane) < n) {
-            uint32_t const entry = ws.defer[lane];
-            key = full_key(&ws, lut, leaf, entry);
-            consume(key, entry >> 8, ws.seg_info[entry >> 8]);
-        }
-        fold(key);
-        uint32_t const rem = queued - n;
-        uint32_t t = 0;
-        __syncwarp();
-        if (uint32_t(lane) < rem) t = ws.defer[n + lane];
-        __syncwarp();
-        if (uint32_t(lane) < rem) ws.defer[lane] = t;
-        __syncwarp();
-    };
-    uint32_t queued = 0;
-    int seg = 0;
-    // TA3B_ILP candidates per lane per iteration (c, c+32, ...) in straight-line
-    // code, so their dependency chains interleave; out-of-range slots evaluate
-    // the last real candidate and are discarded. 1 measured fastest on B200: 486 ms
-    // per full-generation step vs 681 ms for 2 (no spills at 16 warps per SM) and
-    // 766 ms for 2 at 12 warps per SM.
-    for (uint32_t c0 = 0; c0 < total; c0 += TA3B_ILP * WARP) {
-        uint32_t info[TA3B_ILP], idx[TA3B_ILP], sg[TA3B_ILP];
-        bool valid[TA3B_ILP];
-#pragma unroll
-        for (int u = 0; u < TA3B_ILP; ++u) {
-            uint32_t const c = c0 + uint32_t(u * WARP + lane);
-            valid[u] = c < total;
-            uint32_t const cc = valid[u] ? c : total - 1u;
-            while (ws.seg_off[seg + 1] <= cc) ++seg;
-            sg[u] = uint32_t(seg);
-            info[u] = ws.seg_info[seg];
-            idx[u] = cc - ws.seg_off[seg];
-        }
-        float v[TA3B_ILP];
-        int st[TA3B_ILP];
-#pragma unroll
-        for (int u = 0; u < TA3B_ILP; ++u) {
-            if constexpr (WIDE)
-                st[u] = fast_candidate_wide<HW>(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
-                                                (info[u] >> 20) & 1u, ws.wglobal, hb, lane, v[u]);
-            else
-                st[u] = fast_candidate(ws.rec[info[u] & 63u], lut.fast[(info[u] >> 16) & 7u][idx[u]],
-                                       (info[u] >> 20) & 1u, fw, v[u]);
-        }
-#pragma unroll
-        for (int u = 0; u < TA3B_ILP; ++u) {
-            uint64_t key = 0;
-            bool const def = valid[u] && st[u] != FAST_OK;
-            if (valid[u] && st[u] == FAST_OK) {
-                key = candidate_key(leaf, v[u], info[u], idx[u]);
-                consume(key, sg[u], info[u]);
-            }
-            uint32_t const dm = __ballot_sync(FULL_MASK, def);
-            if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = (sg[u] << 8) | idx[u];
-            queued += __popc(dm);
-            fold(key);
-            if (queued >= uint32_t(WARP)) {
-                __syncwarp();
-                drain(WARP, queued);
-                queued -= WARP;
-            }
-        }
-    }
-    __syncwarp();
-    while (queued) {
-        uint32_t const n = queued < uint32_t(WARP) ? queued : uint32_t(WARP);
-        drain(n, queued);
-        queued -= n;
     }
     return acc;
 }
@@ -689,10 +682,6 @@ __device__ __forceinline__ uint32_t build_segments(WarpShared& ws, uint32_t cons
     return base;
 }
 
-#ifndef TA3B_ONE_BUILDER
-#define TA3B_ONE_BUILDER 0
-#endif
-
 // lane j builds kept node j (when active): parent record `prec`, placement (piece, i); with
 // root, the active lane builds record 32 from the committed board (no placement, no clears)
 template <bool WIDE>
@@ -716,19 +705,12 @@ __device__ __noinline__ void materialize(WarpShared* ws, Luts lut, bool active, 
     __syncwarp();
 }
 
-// the committed board's record (record 32): one lane builds it, the warp waits
+// the committed board's record (record 32): one lane builds it through materialize's body, so the
+// kernel holds one copy of the record builder (a second inlined copy measured 5 % slower on the
+// headline generation: the kernel is bound by instruction fetch as much as by issue)
 template <bool WIDE>
-__device__ __noinline__ void root_record(WarpShared* ws, Luts lut, int lane) {
-#if TA3B_ONE_BUILDER
-    materialize<WIDE>(ws, lut, lane == 0, 0u, 0u, 0u, lane, true);       // the same record-builder body
-#else
-    if (lane == 0) {
-        uint32_t b[W];
-        load_board(ws->eng.board, b);
-        build_record<SmemW, !WIDE>(b, 0u, SmemW{ws->wfull}, ws->rec[32]);
-    }
-    __syncwarp();
-#endif
+__device__ __forceinline__ void root_record(WarpShared* ws, Luts lut, int lane) {
+    materialize<WIDE>(ws, lut, lane == 0, 0u, 0u, 0u, lane, true);
 }
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game
@@ -930,8 +912,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                     t[2] = uint8_t(mv.x + 2);
                 }
                 if (mv.hold) engine_hold(ws.eng);
-                int const cl = engine_place(ws.eng, mv.orient, mv.x);
-                if (cl >= 0) stats_advance(ws.st, ws.eng.board, uint32_t(cl));
+                BoardInts bi;
+                int const cl = engine_place(ws.eng, mv.orient, mv.x, bi);
+                if (cl >= 0) stats_advance(ws.st, bi, uint32_t(cl));
                 else ws.eng.over = 2;                                // DIED: stop without a stats update
             }
             ++moves;
