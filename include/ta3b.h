@@ -184,9 +184,14 @@ int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out);
 
 /* Kernel launch-shape variants (warps per block x register cap expressed as
  * minimum resident blocks per SM): the autotuner's search space. No reference
- * counterpart (the reference has one fixed launch, model_eval.cu:143). */
+ * counterpart (the reference has one fixed launch, model_eval.cu:143).
+ * ta3b_variant_warps_per_game: 1 for the single-warp kernels, 2 for the paired
+ * kernels (two warps share every game's candidate passes; same results bit for
+ * bit), -1 for a variant out of range. ta3b_config's warps_per_block /
+ * blocks_per_sm select among the single-warp variants only. */
 int ta3b_num_variants(void);
 int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm);
+int ta3b_variant_warps_per_game(int variant);
 int ta3b_select_variant(ta3b_ctx* ctx, int variant);
 
 /* Device self-test of the per-candidate evaluation (tests and tooling): one

@@ -56,8 +56,12 @@ def test_variants_enumerate(lib):
     from tetris_ai3_b200 import ModelEvaluator
     v = ModelEvaluator.variants()
     assert len(v) == lib.ta3b_num_variants() >= 2
-    assert all(x["warps_per_block"] in (2, 4, 8, 10, 16, 20) for x in v)
-    assert {x["warps_per_block"] for x in v} == {2, 4, 8, 10, 16, 20}
+    solo = [x for x in v if x["warps_per_game"] == 1]
+    pair = [x for x in v if x["warps_per_game"] == 2]
+    assert len(solo) + len(pair) == len(v) and pair
+    assert {x["warps_per_block"] for x in solo} == {2, 4, 8, 10, 16, 20}
+    assert all(x["warps_per_block"] % 2 == 0 for x in pair)
+    assert lib.ta3b_variant_warps_per_game(-1) == -1 and lib.ta3b_variant_warps_per_game(len(v)) == -1
 
 
 def _has_gpu():

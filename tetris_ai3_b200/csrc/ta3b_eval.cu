@@ -444,6 +444,44 @@ __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
     return v;
 }
 
+// ----------------------------------------------------------------- pairs ---
+// Paired kernels play every game with two warps of a block: the even warp (the leader) owns
+// the game and runs everything but the candidate passes alone; in each stage the two warps
+// take alternate 32-candidate rounds (leader rounds 0, 2, 4, ..., partner 1, 3, 5, ...), each
+// keeps its own top-K list, argmax, legality bits and evaluation count, and the leader merges
+// the partner's (keys are unique within a stage, so the result is the single-warp one). A game
+// therefore runs faster while the issue work per move stays the same, which shortens a launch's
+// tail of long games. The two warps synchronise through a counter barrier in shared memory
+// whose wait gives up after kPairWaitNs (no legitimate wait comes near it): the warp sets
+// status bit STATUS_PAIR and leaves, and the call reports TA3B_ERR_DEVICE.
+constexpr uint32_t PAIR_GAME_END = 0xFFFFFFFFu;
+constexpr unsigned long long kPairWaitNs = 1000000000ull;    // 1 s
+constexpr uint32_t STATUS_PAIR = 4u;
+// the partner's stage results, in its own (unused) record area
+constexpr int X_BEST = 32, X_BITS = 33, X_EVALS = 34;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bitonic merge of two descending 32-key lists (lane i = i-th largest) into the top kl keys.
+__device__ __forceinline__ uint64_t shfl64_xor(uint64_t v, int m) {
+    return (uint64_t(__shfl_xor_sync(FULL_MASK, uint32_t(v >> 32), m)) << 32) | __shfl_xor_sync(FULL_MASK, uint32_t(v), m);
+}
+__device__ __forceinline__ uint64_t merge_topk(uint64_t a, uint64_t b, int kl, int lane) {
+    uint64_t const rb = shfl64(b, 31 - lane);                    // ascending
+    uint64_t c = a > rb ? a : rb;                                // bitonic, holds the 32 largest of both
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        uint64_t const o = shfl64_xor(c, j);
+        bool const lower = (lane & j) == 0;
+        c = lower ? (c > o ? c : o) : (c < o ? c : o);
+    }
+    return lane < kl ? c : 0ull;
+}
+
 // ---------------------------------------------------------------- kernel ---
 struct alignas(16) WarpShared {
     uint32_t rec[33][REC_WORDS];      // kept frontier records (rank -> record); [32] = committed board
@@ -455,8 +493,47 @@ struct alignas(16) WarpShared {
     uint32_t seg_off[65];              // a level's candidate segments (parent rank, child list)
     uint32_t seg_info[64];             // rec (6) | rank k << 8 | piece << 16 | held-is-I << 20 | child << 21
     uint32_t defer[64];                // queued (segment << 8 | placement) for the full path
+    // paired kernels (two warps per game; the game lives in the even warp's area)
+    uint32_t pair_ctr;                 // this warp's barrier count
+    uint32_t pair_cmd;                 // game area: the stage to run next, or PAIR_GAME_END
+    uint32_t pair_total;               // game area: that stage's candidate count
+    uint32_t pair_sim;                 // game area: the sim the pair plays (kNoSim: none left)
+    uint32_t pair_broken;              // this warp: a pair wait ran out
+    uint32_t pad_pair_[3];
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte alignment");
+
+// The pair barrier (pr[0] the leader's area, pr[1] the partner's): each warp counts its arrivals
+// in its own word and waits until its mate's count has caught up, so a warp runs at most one
+// barrier ahead. Writes before the barrier are visible to the mate after it. false: the wait ran
+// out (status bit set, this warp's pair_broken set).
+__device__ __forceinline__ bool pair_sync(WarpShared* pr, bool partner, uint32_t* status, int lane) {
+    WarpShared& me = pr[partner ? 1 : 0];
+    int ok = 1;
+    __syncwarp();
+    if (lane == 0) {
+        __threadfence_block();
+        uint32_t const mine = me.pair_ctr + 1u;
+        *reinterpret_cast<volatile uint32_t*>(&me.pair_ctr) = mine;
+        volatile uint32_t const* const other = &pr[partner ? 0 : 1].pair_ctr;
+        if (int(*other - mine) < 0) {
+            unsigned long long const t0 = global_ns();
+            while (int(*other - mine) < 0) {
+                __nanosleep(20);
+                if (global_ns() - t0 > kPairWaitNs) {
+                    atomicOr(status, STATUS_PAIR);
+                    me.pair_broken = 1u;
+                    ok = 0;
+                    break;
+                }
+            }
+        }
+        __threadfence_block();
+    }
+    ok = __shfl_sync(FULL_MASK, ok, 0);
+    __syncwarp();
+    return ok != 0;
+}
 
 struct Params {
     float const* weights;
@@ -552,10 +629,12 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // One level: every candidate of the segment table, on the fast path or queued
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
-// per-parent legality.
-template <int NET, bool KEYS>
-__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW const& fw, float* hb, bool leaf,
-                                               uint32_t total, int kl, int lane, uint32_t& evals) {
+// per-parent legality. ws is the game's area, dq the warp's own queue of deferred candidates.
+// PAIR: this warp takes every other 32-candidate round, starting at candidate `first`.
+template <int NET, bool KEYS, bool PAIR = false>
+__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* dq, Luts lut, FastW const& fw, float* hb,
+                                               bool leaf, uint32_t total, int kl, int lane, uint32_t& evals,
+                                               uint32_t first = 0) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
     LevelAcc acc{0, 0, 0, 0, 0, 0};
@@ -575,7 +654,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
     // per lane in straight-line code measured slower (681 ms vs 486 ms per full generation).
     uint32_t queued = 0;          // < 32 at the start of every fast round: the queue holds 64
     int seg = 0;
-    uint32_t c0 = 0;
+    uint32_t c0 = PAIR ? first : 0u;
     for (;;) {
         bool const more = c0 < total;
         if (!more && queued == 0) break;
@@ -590,7 +669,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
                 uint32_t entry = 0;
                 bool legal = false;
                 if (uint32_t(lane) < n) {
-                    entry = ws.defer[lane];
+                    entry = dq[lane];
                     legal = full_inputs_wide(&ws, lut, entry, in);
                     if (!legal) in = WideIn{};
                 }
@@ -602,16 +681,16 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
                     consume(key, entry >> 8, info);
                 }
             } else if (uint32_t(lane) < n) {
-                uint32_t const entry = ws.defer[lane];
+                uint32_t const entry = dq[lane];
                 key = full_key(&ws, lut, leaf, entry);
                 consume(key, entry >> 8, ws.seg_info[entry >> 8]);
             }
             uint32_t const rem = queued - n;
             uint32_t t = 0;
             __syncwarp();
-            if (uint32_t(lane) < rem) t = ws.defer[n + lane];
+            if (uint32_t(lane) < rem) t = dq[n + lane];
             __syncwarp();
-            if (uint32_t(lane) < rem) ws.defer[lane] = t;
+            if (uint32_t(lane) < rem) dq[lane] = t;
             __syncwarp();
             queued = rem;
         } else {
@@ -636,9 +715,9 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, Luts lut, FastW c
                 consume(key, sg, info);
             }
             uint32_t const dm = __ballot_sync(FULL_MASK, def);
-            if (def) ws.defer[queued + __popc(dm & ((1u << lane) - 1u))] = (sg << 8) | idx;
+            if (def) dq[queued + __popc(dm & ((1u << lane) - 1u))] = (sg << 8) | idx;
             queued += __popc(dm);
-            c0 += WARP;
+            c0 += PAIR ? 2u * WARP : uint32_t(WARP);
         }
         if (leaf) {
             if (KEYS) top2_insert(acc.best, acc.best2, key);
@@ -713,32 +792,51 @@ __device__ __forceinline__ void root_record(WarpShared* ws, Luts lut, int lane) 
     materialize<WIDE>(ws, lut, lane == 0, 0u, 0u, 0u, lane, true);
 }
 
-// search_move_beam (beam.hpp:484-570) for the warp's committed game
-template <int NET, bool KEYS>
+// search_move_beam (beam.hpp:484-570) for the warp's committed game.
+// PAIR: ws is the pair's game (the leader's area, the partner's follows it). The leader runs the
+// search and posts each stage; the partner stays in here for the whole game, runs the stages it
+// is posted (its half of each candidate pass) and returns when the leader posts PAIR_GAME_END.
+template <int NET, bool KEYS, bool PAIR = false>
 __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
     constexpr bool WIDE = NET != 0;
+    static_assert(!PAIR || (!WIDE && !KEYS), "paired kernels run the v11 model without key tracing");
+    bool const partner = PAIR && (threadIdx.x & 32u) != 0;
+    WarpShared* const pr = &ws;
     Move mv{0, 0, 0, true, 0, 0};
-    if (ws.eng.over) return mv;
+    if (!partner && ws.eng.over) return mv;
     uint32_t slot_piece[NSLOTS];                                  // beam.hpp:226-237
-    slot_piece[0] = ws.eng.held;
-    slot_piece[1] = ws.eng.queue[0];
+    int tree = 0;
+    uint32_t r0 = 0, r1 = 0, p0 = 0, p1 = 0;
+    if (!partner) {
+        slot_piece[0] = ws.eng.held;
+        slot_piece[1] = ws.eng.queue[0];
 #pragma unroll
-    for (int i = 0; i < DEPTH; ++i) slot_piece[2 + i] = ws.eng.queue[1 + i];
-    int const tree = ws.eng.held == NO_PIECE ? 1 : 0;
-    uint32_t const r0 = c_tables.node[tree][0][0], r1 = c_tables.node[tree][0][1];
-    uint32_t const p0 = slot_piece[r0 & 0xFu], p1 = slot_piece[r1 & 0xFu];
+        for (int i = 0; i < DEPTH; ++i) slot_piece[2 + i] = ws.eng.queue[1 + i];
+        tree = ws.eng.held == NO_PIECE ? 1 : 0;
+        r0 = c_tables.node[tree][0][0];
+        r1 = c_tables.node[tree][0][1];
+        p0 = slot_piece[r0 & 0xFu];
+        p1 = slot_piece[r1 & 0xFu];
+    }
 
     int kept = 1;                              // frontier size feeding the next stage
     uint32_t fscore = 0, fnode = 0, frank = uint32_t(lane), root_slot = 0;
     uint64_t best = 0;                         // leaf-order (score | order) maximum, fallbacks included
     uint64_t best2 = 0;                        // the second-largest such key (tracing flavour)
 #pragma unroll 1
-    for (int stage = 0; stage < DEPTH; ++stage) {
-        bool const leaf = stage == DEPTH - 1;
+    for (int stage = 0;; ++stage) {
         // ---- segments of this stage
         uint32_t total;
-        if (stage == 0) {                      // two root groups over the committed board (beam.hpp:283-301)
+        if (partner) {                         // the stage the leader posts, or the end of the game
+            if (!pair_sync(pr, true, status, lane)) return mv;
+            uint32_t const cmd = ws.pair_cmd;
+            if (cmd == PAIR_GAME_END) return mv;
+            stage = int(cmd);
+            total = ws.pair_total;
+        } else if (stage == DEPTH) {
+            break;
+        } else if (stage == 0) {               // two root groups over the committed board (beam.hpp:283-301)
             root_record<WIDE>(&ws, lut, lane);
             if (lane < 2) {
                 uint32_t const nd = lane ? r1 : r0;
@@ -757,9 +855,40 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         } else {
             total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
+        if (PAIR && !partner) {                // post the stage
+            if (lane == 0) {
+                ws.pair_cmd = uint32_t(stage);
+                ws.pair_total = total;
+            }
+            if (!pair_sync(pr, false, status, lane)) return mv;
+        }
+        bool const leaf = stage == DEPTH - 1;
+        int const kl = stage == 0 ? K0 : (stage == 1 ? K1 : K2);
         // ---- every candidate of the stage
-        LevelAcc const a = level_pass<NET, KEYS>(ws, lut, fw, hb, leaf, total,
-                                                   stage == 0 ? K0 : (stage == 1 ? K1 : K2), lane, evals);
+        LevelAcc a = level_pass<NET, KEYS, PAIR>(ws, pr[partner ? 1 : 0].defer, lut, fw, hb, leaf, total, kl, lane,
+                                                 evals, partner ? uint32_t(WARP) : 0u);
+        if (PAIR) {
+            // the partner's results go through its own record area, which it never uses otherwise:
+            // its list (or per-lane argmax) in words 0-63, its legality bits in words 64-65
+            uint32_t* const x = pr[1].rec[0];
+            uint64_t* const xk = reinterpret_cast<uint64_t*>(x);
+            if (partner) {
+                xk[lane] = leaf ? a.best : a.list;
+                uint32_t const lo = __reduce_or_sync(FULL_MASK, a.lo), hi = __reduce_or_sync(FULL_MASK, a.hi);
+                if (lane == 0) {
+                    x[64] = lo;
+                    x[65] = hi;
+                }
+                if (!pair_sync(pr, true, status, lane)) return mv;
+                continue;
+            }
+            if (!pair_sync(pr, false, status, lane)) return mv;
+            uint64_t const b = xk[lane];
+            if (leaf) a.best = b > a.best ? b : a.best;
+            else a.list = merge_topk(a.list, b, kl, lane);
+            a.lo |= x[64];
+            a.hi |= x[65];
+        }
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
             kept = __popc(__ballot_sync(FULL_MASK, a.list != 0));
@@ -845,20 +974,31 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
 // BUDGET: the flavour that checks the launch's time budget after every move (a separate
 // instantiation: the check's registers would otherwise cost the ordinary kernels spills).
 // KEYS: the tracing flavour that also records each move's two largest final keys (p.keys).
-template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false>
+// PAIR: two warps per game (v11 only, no budget, no key tracing): the even warp of each pair
+// takes the tickets, commits the moves and writes the results, the odd warp runs half of every
+// candidate pass (search_move's PAIR mode); results are the single-warp kernel's, bit for bit.
+template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false, bool PAIR = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;
+    static_assert(!PAIR || (!WIDE && !BUDGET && !KEYS && WARPS % 2 == 0), "paired kernels: v11, whole pairs");
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
     for (int t = int(threadIdx.x); t < NPIECE * MP; t += WARPS * 32) {
         s_lut.fast[t / MP][t % MP] = g_lut.fast[t / MP][t % MP];
         s_lut.move[t / MP][t % MP] = g_lut.move[t / MP][t % MP];
     }
+    int const lane = int(threadIdx.x & 31u);
+    bool const partner = PAIR && (threadIdx.x & 32u) != 0;
+    // PAIR: pr[0] is the pair's game (the leader's area), pr[1] the partner's area
+    WarpShared* const pr = reinterpret_cast<WarpShared*>(dyn_smem) + (PAIR ? (threadIdx.x >> 5) & ~1u : threadIdx.x >> 5);
+    WarpShared& ws = pr[0];
+    if (PAIR && lane == 0) {
+        pr[partner ? 1 : 0].pair_ctr = 0;
+        pr[partner ? 1 : 0].pair_broken = 0;
+    }
     __syncthreads();
     Luts const lut{s_lut.fast, s_lut.move};
-    int const lane = int(threadIdx.x & 31u);
-    WarpShared& ws = reinterpret_cast<WarpShared*>(dyn_smem)[threadIdx.x >> 5];
     // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
     float* const hb = WIDE ? reinterpret_cast<float*>(dyn_smem + WARPS * sizeof(WarpShared)) +
                                  (threadIdx.x >> 5) * kWideHbFloats<HW>
@@ -870,11 +1010,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         // a 64-bit ticket: every resident warp draws one past the last sim, which a 32-bit
         // counter could wrap near 2^32 sims; kNoSim (no sim index is that large) ends the warp
         uint32_t sim = 0;
-        if (lane == 0) {
+        if (!partner && lane == 0) {
             unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
             sim = t < p.total_sims ? uint32_t(t) : kNoSim;
         }
-        sim = __shfl_sync(FULL_MASK, sim, 0);
+        if (PAIR) {                                                // the leader hands the sim to its partner
+            if (!partner && lane == 0) ws.pair_sim = sim;
+            if (!pair_sync(pr, partner, &p.scratch[kStatusWord], lane)) break;
+            sim = __shfl_sync(FULL_MASK, ws.pair_sim, 0);
+        } else {
+            sim = __shfl_sync(FULL_MASK, sim, 0);
+        }
         if (sim == kNoSim) break;
         uint32_t const mdl = sim / p.num_games, g = sim % p.num_games;
         uint32_t const island = mdl / p.models_per_island;
@@ -886,19 +1032,28 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             p.timing[2 * size_t(sim)] = t;
         }
         FastW fw;
-        if (!WIDE) {
-            load_fast_weights(GlobalW{wsrc}, fw);
-            for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
+        uint32_t evals = 0, moves = 0;
+        if (!WIDE) load_fast_weights(GlobalW{wsrc}, fw);
+        if (partner) {
+            // serve the leader's stages until the game ends, then hand over the evaluation count
+            search_move<NET, KEYS, PAIR>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            if (pr[1].pair_broken) break;
+            evals = __reduce_add_sync(FULL_MASK, evals);
+            if (lane == 0) pr[1].rec[0][66] = evals;
+            if (!pair_sync(pr, true, &p.scratch[kStatusWord], lane)) break;
+            continue;
         }
+        if (!WIDE)
+            for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
         if (lane == 0) {
             ws.wglobal = wsrc;
             engine_reset(ws.eng, seed);
             ws.st = Stats{};
         }
         __syncwarp();
-        uint32_t evals = 0, moves = 0;
         for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move<NET, KEYS>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            Move const mv = search_move<NET, KEYS, PAIR>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            if (PAIR && ws.pair_broken) break;
             if (KEYS && lane == 0 && p.keys) {
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2] = mv.key1;
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2 + 1] = mv.key2;
@@ -933,7 +1088,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (ws.eng.over == 3) break;
             }
         }
+        if (PAIR) {                                                // end the partner's game, take its count
+            if (ws.pair_broken) break;
+            if (lane == 0) ws.pair_cmd = PAIR_GAME_END;
+            if (!pair_sync(pr, false, &p.scratch[kStatusWord], lane)) break;
+            if (!pair_sync(pr, false, &p.scratch[kStatusWord], lane)) break;
+        }
         evals = __reduce_add_sync(FULL_MASK, evals);
+        if (PAIR) evals += pr[1].rec[0][66];
         if (lane == 0) {
             p.score[sim] = final_score(ws.st);
             if (p.pieces) p.pieces[sim] = ws.st.pieces;
@@ -1016,6 +1178,8 @@ using KernelFn = void (*)(Params);
 struct Variant {
     KernelFn fn;
     uint32_t warps, min_blocks;
+    bool pair = false;                 // two warps per game (eval_pair_kernel)
+    uint32_t games() const { return pair ? warps / 2 : warps; }
 };
 Variant const kVariants[] = {
     {eval_kernel<4, 3>, 4, 3}, {eval_kernel<4, 4>, 4, 4}, {eval_kernel<4, 5>, 4, 5}, {eval_kernel<4, 6>, 4, 6},
@@ -1024,6 +1188,8 @@ Variant const kVariants[] = {
     {eval_kernel<8, 2>, 8, 2}, {eval_kernel<16, 1>, 16, 1},
     // 20 warps per SM (the 68-word records leave room for them) at a ~100-register cap
     {eval_kernel<10, 2>, 10, 2}, {eval_kernel<20, 1>, 20, 1},
+    // two warps per game: 6 games per SM at a 168-register cap, 4 games per SM uncapped
+    {eval_kernel<12, 1, 0, false, false, true>, 12, 1, true}, {eval_kernel<8, 1, 0, false, false, true>, 8, 1, true},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // the networks a launch can run: v11, or the widened 10 -> H -> H -> 1 for H = 64 or 32
@@ -1205,11 +1371,11 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     Variant const* const v = keys     ? &kKeysNet[ni]
                              : budget ? &kBudgetNet[ni]
                              : ni != NET_V11 ? &kWideNet[ni] : &kVariants[ctx->variant];
-    uint32_t const warps = v->warps;
+    uint32_t const warps = v->warps, games = v->games();
     uint32_t const max_grid = keys     ? ctx->keys_grid[ni]
                               : budget ? ctx->budget_grid[ni]
                               : ni != NET_V11 ? ctx->net_grid[ni] : ctx->grid;
-    uint32_t const need_blocks = (prm.total_sims + warps - 1) / warps;
+    uint32_t const need_blocks = (prm.total_sims + games - 1) / games;
     uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
     Params p2 = prm;
     p2.budget_ns = ctx->budget_ns;
@@ -1395,7 +1561,7 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
     if (c.warps_per_block || c.blocks_per_sm) {
         v = -1;
         for (int i = 0; i < kNumVariants; ++i)
-            if ((!c.warps_per_block || kVariants[i].warps == c.warps_per_block) &&
+            if (!kVariants[i].pair && (!c.warps_per_block || kVariants[i].warps == c.warps_per_block) &&
                 (!c.blocks_per_sm || kVariants[i].min_blocks == c.blocks_per_sm)) {
                 v = i;
                 break;
@@ -1542,6 +1708,11 @@ int ta3b_core_selftest(uint32_t const* recs, uint32_t num_recs, uint32_t const* 
 }
 
 int ta3b_num_variants(void) { return kNumVariants; }
+
+int ta3b_variant_warps_per_game(int variant) {
+    if (variant < 0 || variant >= kNumVariants) return -1;
+    return kVariants[variant].pair ? 2 : 1;
+}
 
 int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm) {
     if (variant < 0 || variant >= kNumVariants) return TA3B_ERR_ARG;

@@ -32,6 +32,7 @@ _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
            "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
+           "ta3b_variant_warps_per_game",
            "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc", "ta3b_set_time_budget",
            "ta3b_device_status", "ta3b_noalloc_status"]
 
@@ -68,6 +69,7 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_launch_info.argtypes = [vp, vp, vp, vp]
     lib.ta3b_num_variants.argtypes = []
     lib.ta3b_variant_info.argtypes = [C.c_int, vp, vp]
+    lib.ta3b_variant_warps_per_game.argtypes = [C.c_int]
     lib.ta3b_select_variant.argtypes = [vp, C.c_int]
     lib.ta3b_set_time_budget.argtypes = [vp, C.c_double]
     lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
@@ -267,7 +269,8 @@ class ModelEvaluator:
         for v in range(lib.ta3b_num_variants()):
             w, b = C.c_uint32(), C.c_uint32()
             lib.ta3b_variant_info(v, C.byref(w), C.byref(b))
-            out.append({"variant": v, "warps_per_block": w.value, "min_blocks_per_sm": b.value})
+            out.append({"variant": v, "warps_per_block": w.value, "min_blocks_per_sm": b.value,
+                        "warps_per_game": lib.ta3b_variant_warps_per_game(v)})
         return out
 
     def autotune(self, weights, seeds, max_moves: int, score, pieces=None, lines=None, evals=None,
