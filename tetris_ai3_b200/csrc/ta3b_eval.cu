@@ -414,27 +414,6 @@ __device__ __forceinline__ uint64_t shfl64_up(uint64_t v) {
     return (uint64_t(__shfl_up_sync(FULL_MASK, uint32_t(v >> 32), 1)) << 32) | __shfl_up_sync(FULL_MASK, uint32_t(v), 1);
 }
 
-// Fold one key per lane into the warp's sorted top-K list (lane i = i-th
-// largest, 0 = empty; `thr` caches list[k-1]). Keys are unique per level (the
-// low word encodes the slot), so the kept set equals beam.hpp:244-265's "max
-// score, lowest slot on ties" whatever the order keys arrive in. (A bitonic
-// sort-and-merge of whole rounds measured slower than these insertions.)
-__device__ __forceinline__ void topk_fold(uint64_t& list, uint64_t& thr, uint64_t key, int k, int lane) {
-    uint32_t mask = __ballot_sync(FULL_MASK, key > thr);
-    if (!mask) return;
-    while (mask) {
-        int const s = __ffs(int(mask)) - 1;
-        uint64_t const x = shfl64(key, s);
-        int const pos = __popc(__ballot_sync(FULL_MASK, list > x));
-        uint64_t const up = shfl64_up(list);
-        if (lane > pos && lane < k) list = up;
-        if (lane == pos) list = x;
-        thr = shfl64(list, k - 1);
-        mask &= ~(1u << s);
-        mask &= __ballot_sync(FULL_MASK, key > thr);
-    }
-}
-
 __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -466,10 +445,25 @@ __device__ __forceinline__ unsigned long long global_ns() {
     return t;
 }
 
-// Bitonic merge of two descending 32-key lists (lane i = i-th largest) into the top kl keys.
 __device__ __forceinline__ uint64_t shfl64_xor(uint64_t v, int m) {
     return (uint64_t(__shfl_xor_sync(FULL_MASK, uint32_t(v >> 32), m)) << 32) | __shfl_xor_sync(FULL_MASK, uint32_t(v), m);
 }
+
+// Bitonic sort of one key per lane into descending order (lane i = i-th largest).
+__device__ __forceinline__ uint64_t warp_sort_desc(uint64_t v, int lane) {
+#pragma unroll
+    for (int k = 2; k <= WARP; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            uint64_t const o = shfl64_xor(v, j);
+            bool const keep_max = ((lane & j) == 0) == ((lane & k) == 0);   // descending runs where lane & k == 0
+            v = keep_max ? (v > o ? v : o) : (v < o ? v : o);
+        }
+    }
+    return v;
+}
+
+// Bitonic merge of two descending 32-key lists (lane i = i-th largest) into the top kl keys.
 __device__ __forceinline__ uint64_t merge_topk(uint64_t a, uint64_t b, int kl, int lane) {
     uint64_t const rb = shfl64(b, 31 - lane);                    // ascending
     uint64_t c = a > rb ? a : rb;                                // bitonic, holds the 32 largest of both
@@ -493,42 +487,51 @@ struct alignas(16) WarpShared {
     uint32_t seg_off[65];              // a level's candidate segments (parent rank, child list)
     uint32_t seg_info[64];             // rec (6) | rank k << 8 | piece << 16 | held-is-I << 20 | child << 21
     uint32_t defer[64];                // queued (segment << 8 | placement) for the full path
+    alignas(8) uint64_t kbuf[WARP];    // a level's keys above the top-K threshold, not yet merged
     // paired kernels (two warps per game; the game lives in the even warp's area)
-    uint32_t pair_ctr;                 // this warp's barrier count
+    alignas(8) unsigned long long pair_bar;   // game area: the pair's barrier (an mbarrier of 2 arrivals)
     uint32_t pair_cmd;                 // game area: the stage to run next, or PAIR_GAME_END
     uint32_t pair_total;               // game area: that stage's candidate count
     uint32_t pair_sim;                 // game area: the sim the pair plays (kNoSim: none left)
     uint32_t pair_broken;              // this warp: a pair wait ran out
-    uint32_t pad_pair_[3];
+    uint32_t pad_pair_[2];
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte alignment");
 
-// The pair barrier (pr[0] the leader's area, pr[1] the partner's): each warp counts its arrivals
-// in its own word and waits until its mate's count has caught up, so a warp runs at most one
-// barrier ahead. Writes before the barrier are visible to the mate after it. false: the wait ran
-// out (status bit set, this warp's pair_broken set).
+// The pair barrier (pr[0] the leader's area, pr[1] the partner's): an mbarrier in the game area
+// that completes a phase when both warps' lane 0 have arrived. Arrival releases and the wait
+// acquires, so the warps' shared-memory writes before the barrier are visible to the mate after
+// it. The wait polls mbarrier.try_wait (which suspends the thread in hardware between polls) and
+// gives up after kPairWaitNs: false = it ran out (status bit set, this warp's pair_broken set).
+__device__ __forceinline__ void pair_bar_init(WarpShared* pr) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(uint32_t(__cvta_generic_to_shared(&pr[0].pair_bar)))
+                 : "memory");
+}
+
 __device__ __forceinline__ bool pair_sync(WarpShared* pr, bool partner, uint32_t* status, int lane) {
-    WarpShared& me = pr[partner ? 1 : 0];
     int ok = 1;
     __syncwarp();
     if (lane == 0) {
-        __threadfence_block();
-        uint32_t const mine = me.pair_ctr + 1u;
-        *reinterpret_cast<volatile uint32_t*>(&me.pair_ctr) = mine;
-        volatile uint32_t const* const other = &pr[partner ? 0 : 1].pair_ctr;
-        if (int(*other - mine) < 0) {
-            unsigned long long const t0 = global_ns();
-            while (int(*other - mine) < 0) {
-                __nanosleep(20);
-                if (global_ns() - t0 > kPairWaitNs) {
-                    atomicOr(status, STATUS_PAIR);
-                    me.pair_broken = 1u;
-                    ok = 0;
-                    break;
-                }
+        uint32_t const bar = uint32_t(__cvta_generic_to_shared(&pr[0].pair_bar));
+        unsigned long long state;
+        asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(bar) : "memory");
+        unsigned long long t0 = 0;
+        for (uint32_t polls = 0;; ++polls) {
+            uint32_t done;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(bar), "l"(state)
+                : "memory");
+            if (done) break;
+            if (polls == 0) t0 = global_ns();
+            else if ((polls & 15u) == 0 && global_ns() - t0 > kPairWaitNs) {
+                atomicOr(status, STATUS_PAIR);
+                pr[partner ? 1 : 0].pair_broken = 1u;
+                ok = 0;
+                break;
             }
         }
-        __threadfence_block();
     }
     ok = __shfl_sync(FULL_MASK, ok, 0);
     __syncwarp();
@@ -629,14 +632,24 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // One level: every candidate of the segment table, on the fast path or queued
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
-// per-parent legality. ws is the game's area, dq the warp's own queue of deferred candidates.
+// per-parent legality. ws is the game's area, own the warp's own (its queue of deferred
+// candidates and its key buffer; the same area except in paired kernels).
 // PAIR: this warp takes every other 32-candidate round, starting at candidate `first`.
+//
+// The top-kl list (lane i = i-th largest, 0 = empty; thr = list[kl-1]) is kept lazily: keys
+// above thr go to the warp's key buffer, and when a round's keys would overflow it (or the level
+// ends) the buffer is sorted across the lanes and merged into the list, which raises thr. Keys
+// are unique per level (the low word encodes the slot), so the kept set equals
+// beam.hpp:244-265's "max score, lowest slot on ties" whatever the order keys arrive in; a key at
+// or below a stale thr is below the final list[kl-1] too.
 template <int NET, bool KEYS, bool PAIR = false>
-__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* dq, Luts lut, FastW const& fw, float* hb,
+__device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, Luts lut, FastW const& fw, float* hb,
                                                bool leaf, uint32_t total, int kl, int lane, uint32_t& evals,
                                                uint32_t first = 0) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
+    uint32_t* const dq = own.defer;
+    uint64_t* const kb = own.kbuf;
     LevelAcc acc{0, 0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
@@ -653,13 +666,17 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* dq, Lut
     // code small (the kernel is bound by instruction fetch as much as by issue). Two candidates
     // per lane in straight-line code measured slower (681 ms vs 486 ms per full generation).
     uint32_t queued = 0;          // < 32 at the start of every fast round: the queue holds 64
+    uint32_t kcnt = 0;            // keys in the key buffer (non-leaf levels)
     int seg = 0;
     uint32_t c0 = PAIR ? first : 0u;
     for (;;) {
         bool const more = c0 < total;
-        if (!more && queued == 0) break;
+        // the level's candidates are done; a non-leaf level takes one more turn to merge its buffer
+        bool const fin = !more && queued == 0;
+        if (fin && (leaf || kcnt == 0)) break;
         uint64_t key = 0;
-        if (queued >= uint32_t(WARP) || !more) {
+        if (fin) {
+        } else if (queued >= uint32_t(WARP) || !more) {
             // ---- a batch of deferred candidates through the full reference path
             uint32_t const n = queued < uint32_t(WARP) ? queued : uint32_t(WARP);
             __syncwarp();
@@ -723,7 +740,20 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, uint32_t* dq, Lut
             if (KEYS) top2_insert(acc.best, acc.best2, key);
             else acc.best = key > acc.best ? key : acc.best;
         } else {
-            topk_fold(acc.list, acc.thr, key, kl, lane);
+            uint32_t m = __ballot_sync(FULL_MASK, key > acc.thr);
+            uint32_t n = __popc(m);
+            if (fin || kcnt + n > uint32_t(WARP)) {          // merge the buffer into the list
+                __syncwarp();
+                uint64_t const b = warp_sort_desc(uint32_t(lane) < kcnt ? kb[lane] : 0ull, lane);
+                acc.list = merge_topk(acc.list, b, kl, lane);
+                acc.thr = shfl64(acc.list, kl - 1);
+                kcnt = 0;
+                m = __ballot_sync(FULL_MASK, key > acc.thr);
+                n = __popc(m);
+                __syncwarp();
+            }
+            if (key > acc.thr) kb[kcnt + __popc(m & ((1u << lane) - 1u))] = key;
+            kcnt += n;
         }
     }
     return acc;
@@ -865,7 +895,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         bool const leaf = stage == DEPTH - 1;
         int const kl = stage == 0 ? K0 : (stage == 1 ? K1 : K2);
         // ---- every candidate of the stage
-        LevelAcc a = level_pass<NET, KEYS, PAIR>(ws, pr[partner ? 1 : 0].defer, lut, fw, hb, leaf, total, kl, lane,
+        LevelAcc a = level_pass<NET, KEYS, PAIR>(ws, pr[partner ? 1 : 0], lut, fw, hb, leaf, total, kl, lane,
                                                  evals, partner ? uint32_t(WARP) : 0u);
         if (PAIR) {
             // the partner's results go through its own record area, which it never uses otherwise:
@@ -994,7 +1024,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     WarpShared* const pr = reinterpret_cast<WarpShared*>(dyn_smem) + (PAIR ? (threadIdx.x >> 5) & ~1u : threadIdx.x >> 5);
     WarpShared& ws = pr[0];
     if (PAIR && lane == 0) {
-        pr[partner ? 1 : 0].pair_ctr = 0;
+        if (!partner) pair_bar_init(pr);
         pr[partner ? 1 : 0].pair_broken = 0;
     }
     __syncthreads();
@@ -1034,25 +1064,21 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         FastW fw;
         uint32_t evals = 0, moves = 0;
         if (!WIDE) load_fast_weights(GlobalW{wsrc}, fw);
-        if (partner) {
-            // serve the leader's stages until the game ends, then hand over the evaluation count
-            search_move<NET, KEYS, PAIR>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
-            if (pr[1].pair_broken) break;
-            evals = __reduce_add_sync(FULL_MASK, evals);
-            if (lane == 0) pr[1].rec[0][66] = evals;
-            if (!pair_sync(pr, true, &p.scratch[kStatusWord], lane)) break;
-            continue;
-        }
-        if (!WIDE)
-            for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
-        if (lane == 0) {
-            ws.wglobal = wsrc;
-            engine_reset(ws.eng, seed);
-            ws.st = Stats{};
+        if (!partner) {
+            if (!WIDE)
+                for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
+            if (lane == 0) {
+                ws.wglobal = wsrc;
+                engine_reset(ws.eng, seed);
+                ws.st = Stats{};
+            }
         }
         __syncwarp();
-        for (uint32_t mv_i = 0; mv_i < p.max_moves && !ws.eng.over; ++mv_i) {   // model_eval_host.cpp:39-50
+        // PAIR: the partner's one search_move call serves the whole game (it returns when the
+        // leader ends the game), so both roles run the same copy of the search code
+        for (uint32_t mv_i = 0; partner || (mv_i < p.max_moves && !ws.eng.over); ++mv_i) {   // model_eval_host.cpp:39-50
             Move const mv = search_move<NET, KEYS, PAIR>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            if (partner) break;
             if (PAIR && ws.pair_broken) break;
             if (KEYS && lane == 0 && p.keys) {
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2] = mv.key1;
@@ -1088,11 +1114,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (ws.eng.over == 3) break;
             }
         }
-        if (PAIR) {                                                // end the partner's game, take its count
-            if (ws.pair_broken) break;
-            if (lane == 0) ws.pair_cmd = PAIR_GAME_END;
-            if (!pair_sync(pr, false, &p.scratch[kStatusWord], lane)) break;
-            if (!pair_sync(pr, false, &p.scratch[kStatusWord], lane)) break;
+        if (PAIR) {                           // the leader ends the partner's game and takes its count
+            if (pr[partner ? 1 : 0].pair_broken) break;
+            if (!partner) {
+                if (lane == 0) ws.pair_cmd = PAIR_GAME_END;
+                if (!pair_sync(pr, false, &p.scratch[kStatusWord], lane)) break;
+            } else {
+                uint32_t const own = __reduce_add_sync(FULL_MASK, evals);
+                if (lane == 0) pr[1].rec[0][66] = own;
+            }
+            if (!pair_sync(pr, partner, &p.scratch[kStatusWord], lane)) break;
+            if (partner) continue;
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
         if (PAIR) evals += pr[1].rec[0][66];
