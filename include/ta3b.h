@@ -188,7 +188,12 @@ int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out);
  * ta3b_variant_warps_per_game: 1 for the single-warp kernels, 2 for the paired
  * kernels (two warps share every game's candidate passes; same results bit for
  * bit), -1 for a variant out of range. ta3b_config's warps_per_block /
- * blocks_per_sm select among the single-warp variants only. */
+ * blocks_per_sm select among the single-warp variants only.
+ * Launch shape: a context created with the tuned default runs a batch of at most
+ * 4 games per SM (v11 network, no time budget, no key tracing) on the paired
+ * kernel and every other batch on the default variant; a batch smaller than one
+ * block per SM can hold is spread over all SMs. ta3b_select_variant (or a shape
+ * in ta3b_config) fixes the variant for every batch. */
 int ta3b_num_variants(void);
 int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm);
 int ta3b_variant_warps_per_game(int variant);

@@ -53,6 +53,36 @@ def test_golden_games_bit_exact(ev, golden_games, oracle):
         _check_golden_case(ev, case, oracle)
 
 
+@pytest.fixture(scope="module")
+def ev_solo():
+    from tetris_ai3_b200 import ModelEvaluator
+    e = ModelEvaluator(device=0)
+    e.select_variant(7)                     # the single-warp kernel for every batch size
+    yield e
+    e.close()
+
+
+def test_small_batches_run_on_the_paired_kernel(ev, ev_solo):
+    """A default context plays a batch of at most 4 games per SM with two warps per game, spread one
+    block per SM; a selected variant is kept for every batch. Same bits, same evaluation counts."""
+    from tetris_ai3_b200 import workload
+    b = workload.generation_batch(islands=2, pop=5, games=12, max_moves=300, seed=21)
+    out = ev.eval_trace(b.weights[:10], 10, b.seeds[0], b.max_moves)
+    info = ev.launch_info()
+    assert info["warps_per_block"] == 8 and info["grid"] == min(120, info["sms"])
+    ref = ev_solo.eval_trace(b.weights[:10], 10, b.seeds[0], b.max_moves)
+    assert ev_solo.launch_info()["warps_per_block"] == 16
+    for k in ("score", "pieces", "lines", "evals", "moves", "trace", "board"):
+        assert out[k].tobytes() == ref[k].tobytes(), k
+
+
+def test_golden_games_single_warp_kernel(ev_solo, golden_games):
+    """The golden batches are small, so a default context plays them on the paired kernel; the
+    single-warp kernel plays them bit for bit too."""
+    for case in golden_games["cases"]:
+        _check_golden_case(ev_solo, case)
+
+
 def test_trace_keys_match_oracle(ev, oracle, golden_games):
     """Per move, the device's two largest final keys (the tracing flavour) equal the oracle's bit
     for bit, so every decision's top-two margin is the reference algorithm's; the tracing flavour

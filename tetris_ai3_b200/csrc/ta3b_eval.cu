@@ -414,6 +414,24 @@ __device__ __forceinline__ uint64_t shfl64_up(uint64_t v) {
     return (uint64_t(__shfl_up_sync(FULL_MASK, uint32_t(v >> 32), 1)) << 32) | __shfl_up_sync(FULL_MASK, uint32_t(v), 1);
 }
 
+// Fold one key per lane into the warp's sorted top-K list (lane i = i-th largest, 0 = empty;
+// `thr` caches list[k-1]): the keys above thr are inserted one at a time by ballot/shuffle.
+__device__ __forceinline__ void topk_fold(uint64_t& list, uint64_t& thr, uint64_t key, int k, int lane) {
+    uint32_t mask = __ballot_sync(FULL_MASK, key > thr);
+    if (!mask) return;
+    while (mask) {
+        int const s = __ffs(int(mask)) - 1;
+        uint64_t const x = shfl64(key, s);
+        int const pos = __popc(__ballot_sync(FULL_MASK, list > x));
+        uint64_t const up = shfl64_up(list);
+        if (lane > pos && lane < k) list = up;
+        if (lane == pos) list = x;
+        thr = shfl64(list, k - 1);
+        mask &= ~(1u << s);
+        mask &= __ballot_sync(FULL_MASK, key > thr);
+    }
+}
+
 __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -553,6 +571,8 @@ struct Params {
     unsigned long long* keys;          // tracing flavour: per move the final argmax's two largest keys
     unsigned long long budget_ns;      // 0, or the launch's time budget: past it warps stop and set status bit 2
     uint32_t num_games, models_per_island, max_moves, total_sims;
+    uint32_t warps_active;             // 0, or the warps of each block that play (a batch smaller than
+                                       // the grid's slots is spread over every SM); the rest take no sim
 };
 
 struct Move {
@@ -636,12 +656,15 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // candidates and its key buffer; the same area except in paired kernels).
 // PAIR: this warp takes every other 32-candidate round, starting at candidate `first`.
 //
-// The top-kl list (lane i = i-th largest, 0 = empty; thr = list[kl-1]) is kept lazily: keys
-// above thr go to the warp's key buffer, and when a round's keys would overflow it (or the level
-// ends) the buffer is sorted across the lanes and merged into the list, which raises thr. Keys
-// are unique per level (the low word encodes the slot), so the kept set equals
-// beam.hpp:244-265's "max score, lowest slot on ties" whatever the order keys arrive in; a key at
-// or below a stale thr is below the final list[kl-1] too.
+// The top-kl list (lane i = i-th largest, 0 = empty; thr = list[kl-1]): keys are unique per level
+// (the low word encodes the slot), so the kept set equals beam.hpp:244-265's "max score, lowest
+// slot on ties" whatever the order keys arrive in. The single-warp kernels insert each key above
+// thr at once (topk_fold). The paired kernels keep the list lazily: keys above thr go to the
+// warp's key buffer, and when a round's keys would overflow it (or the level ends) the buffer is
+// sorted across the lanes and merged into the list, which raises thr; a key at or below a stale
+// thr is below the final list[kl-1] too. The lazy merge shortens a warp's critical path (15 %
+// per move for a warp alone on its scheduler) but executes more instructions, which costs 3-5 %
+// at 16 warps per SM, where the single-warp kernels run.
 template <int NET, bool KEYS, bool PAIR = false>
 __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, Luts lut, FastW const& fw, float* hb,
                                                bool leaf, uint32_t total, int kl, int lane, uint32_t& evals,
@@ -650,6 +673,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
     uint32_t* const dq = own.defer;
     uint64_t* const kb = own.kbuf;
+    constexpr bool LAZY = PAIR;
     LevelAcc acc{0, 0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
@@ -673,7 +697,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
         bool const more = c0 < total;
         // the level's candidates are done; a non-leaf level takes one more turn to merge its buffer
         bool const fin = !more && queued == 0;
-        if (fin && (leaf || kcnt == 0)) break;
+        if (fin && (leaf || !LAZY || kcnt == 0)) break;
         uint64_t key = 0;
         if (fin) {
         } else if (queued >= uint32_t(WARP) || !more) {
@@ -739,6 +763,8 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
         if (leaf) {
             if (KEYS) top2_insert(acc.best, acc.best2, key);
             else acc.best = key > acc.best ? key : acc.best;
+        } else if (!LAZY) {
+            topk_fold(acc.list, acc.thr, key, kl, lane);
         } else {
             uint32_t m = __ballot_sync(FULL_MASK, key > acc.thr);
             uint32_t n = __popc(m);
@@ -1041,8 +1067,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         // counter could wrap near 2^32 sims; kNoSim (no sim index is that large) ends the warp
         uint32_t sim = 0;
         if (!partner && lane == 0) {
-            unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
-            sim = t < p.total_sims ? uint32_t(t) : kNoSim;
+            // a warp beyond the block's playing warps takes no ticket (the batch is spread over the SMs)
+            sim = kNoSim;
+            if (!p.warps_active || (threadIdx.x >> 5) < p.warps_active) {
+                unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
+                if (t < p.total_sims) sim = uint32_t(t);
+            }
         }
         if (PAIR) {                                                // the leader hands the sim to its partner
             if (!partner && lane == 0) ws.pair_sim = sim;
@@ -1220,8 +1250,9 @@ Variant const kVariants[] = {
     {eval_kernel<8, 2>, 8, 2}, {eval_kernel<16, 1>, 16, 1},
     // 20 warps per SM (the 68-word records leave room for them) at a ~100-register cap
     {eval_kernel<10, 2>, 10, 2}, {eval_kernel<20, 1>, 20, 1},
-    // two warps per game: 6 games per SM at a 168-register cap, 4 games per SM uncapped
-    {eval_kernel<12, 1, 0, false, false, true>, 12, 1, true}, {eval_kernel<8, 1, 0, false, false, true>, 8, 1, true},
+    // two warps per game, 4 games per block (one block per SM, no register cap): batches of at
+    // most 4 games per SM run on it by default
+    {eval_kernel<8, 1, 0, false, false, true>, 8, 1, true},
 };
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // the networks a launch can run: v11, or the widened 10 -> H -> H -> 1 for H = 64 or 32
@@ -1240,6 +1271,7 @@ Variant const kKeysNet[NUM_NETS] = {{eval_kernel<4, 3, 0, false, true>, 4, 3},
                                     {eval_kernel<4, 2, 64, false, true>, 4, 2},
                                     {eval_kernel<4, 3, 32, false, true>, 4, 3}};
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
+constexpr int kSmallVariant = 10;  // the paired kernel: the default for batches of at most 4 games per SM
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
 } // namespace
@@ -1279,6 +1311,8 @@ struct ta3b_ctx {
     uint32_t net_grid[NUM_NETS] = {0, 0, 0};     // widened-network kernels (by NetKind), set up on first use
     uint32_t budget_grid[NUM_NETS] = {0, 0, 0};  // budget flavours (by NetKind), set up on first use
     uint32_t keys_grid[NUM_NETS] = {0, 0, 0};    // key-tracing flavours (by NetKind), set up on first use
+    bool auto_small = true;                      // small v11 batches run the paired kernel (until a variant is selected)
+    uint32_t small_grid = 0;                     // its grid, set up on first use
     uint64_t* d_keys = nullptr;                  // per move the two largest final keys (tracing)
     size_t cap_keys = 0;
     uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
@@ -1400,16 +1434,31 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, kScratchBytes, st), "reset work queue");
     // with a time budget the budget-checking flavour runs, with key tracing the tracing flavour
     // (which runs without the budget); each has its own fixed launch shape
+    // a v11 batch of at most 4 games per SM runs on the paired kernel (two warps per game), whose
+    // moves take 0.69x the single-warp kernel's time at that load, unless a variant was selected
+    Variant const& small = kVariants[kSmallVariant];
+    bool const use_small = ctx->auto_small && ni == NET_V11 && !keys && !budget &&
+                           prm.total_sims <= ctx->sms * small.games();
+    if (use_small && !ctx->small_grid)
+        if (int rc = setup_kernel(ctx, small, NET_V11, ctx->small_grid, "paired kernel")) return rc;
     Variant const* const v = keys     ? &kKeysNet[ni]
                              : budget ? &kBudgetNet[ni]
-                             : ni != NET_V11 ? &kWideNet[ni] : &kVariants[ctx->variant];
+                             : ni != NET_V11 ? &kWideNet[ni]
+                             : use_small ? &small : &kVariants[ctx->variant];
     uint32_t const warps = v->warps, games = v->games();
     uint32_t const max_grid = keys     ? ctx->keys_grid[ni]
                               : budget ? ctx->budget_grid[ni]
-                              : ni != NET_V11 ? ctx->net_grid[ni] : ctx->grid;
-    uint32_t const need_blocks = (prm.total_sims + games - 1) / games;
-    uint32_t const grid = need_blocks < max_grid ? need_blocks : max_grid;
+                              : ni != NET_V11 ? ctx->net_grid[ni]
+                              : use_small ? ctx->small_grid : ctx->grid;
+    // a batch that one block per SM can hold is spread over every SM, one block each (a game runs
+    // faster on an SM it shares with fewer others), rather than packed into the fewest blocks
+    uint32_t const sims = prm.total_sims;
+    bool const spread = sims < ctx->sms * games && ctx->sms <= max_grid;
+    uint32_t const need_blocks = (sims + games - 1) / games;
+    uint32_t const grid = spread ? (sims < ctx->sms ? (sims ? sims : 1u) : ctx->sms)
+                                 : (need_blocks < max_grid ? need_blocks : max_grid);
     Params p2 = prm;
+    p2.warps_active = spread ? (sims + grid - 1) / grid * (warps / games) : 0u;
     p2.budget_ns = ctx->budget_ns;
     v->fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
@@ -1546,6 +1595,7 @@ int select_variant(ta3b_ctx* ctx, int v) {
               "occupancy");
     if (per_sm < 1) return fail(ctx, TA3B_ERR_CUDA, "kernel variant does not fit on an SM");
     ctx->variant = v;
+    ctx->auto_small = false;
     ctx->warps_per_block = kVariants[v].warps;
     ctx->blocks_per_sm = uint32_t(per_sm);
     ctx->grid = ctx->sms * ctx->blocks_per_sm;
@@ -1609,6 +1659,7 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
         ta3b_destroy(ctx);
         return nullptr;
     }
+    ctx->auto_small = !(c.warps_per_block || c.blocks_per_sm);   // a requested shape is kept for every batch
     return ctx;
 }
 

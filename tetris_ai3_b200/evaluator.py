@@ -276,11 +276,17 @@ class ModelEvaluator:
     def autotune(self, weights, seeds, max_moves: int, score, pieces=None, lines=None, evals=None,
                  num_islands: int = 1, stream=None, reps: int = 1):
         """Time every launch-shape variant on this device batch (CUDA events on
-        `stream`) and keep the fastest. Returns {variant: ms}."""
+        `stream`) and keep the fastest. Returns {variant: ms}. A paired variant is
+        timed only when one block per SM holds the batch (beyond that its games
+        run in waves)."""
         import torch
         times = {}
         st = stream or torch.cuda.current_stream()
-        for v in range(len(self.variants())):
+        sms = self.launch_info()["sms"]
+        for info in self.variants():
+            v = info["variant"]
+            if info["warps_per_game"] > 1 and score.numel() > sms * info["warps_per_block"] // info["warps_per_game"]:
+                continue
             self.select_variant(v)
             with torch.cuda.stream(st):
                 self.eval_device(weights, seeds, max_moves, score, pieces, lines, evals, num_islands, st)  # warm
