@@ -72,8 +72,10 @@ def test_small_batches_run_on_the_paired_kernel(ev, ev_solo):
     assert info["warps_per_block"] == 8 and info["grid"] == min(120, info["sms"])
     ref = ev_solo.eval_trace(b.weights[:10], 10, b.seeds[0], b.max_moves)
     assert ev_solo.launch_info()["warps_per_block"] == 16
-    for k in ("score", "pieces", "lines", "evals", "moves", "trace", "board"):
+    for k in ("score", "pieces", "lines", "evals", "moves", "board"):
         assert out[k].tobytes() == ref[k].tobytes(), k
+    for i, nm in enumerate(out["moves"]):                 # a trace row is defined up to its game's moves
+        assert out["trace"][i][:3 * nm].tobytes() == ref["trace"][i][:3 * nm].tobytes(), i
 
 
 def test_golden_games_single_warp_kernel(ev_solo, golden_games):
