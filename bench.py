@@ -61,7 +61,7 @@ HIDDEN = {"wide": 64, "wide32": 32}           # the widened models' hidden width
 # What this kernel executes per placement (ncu thread_inst_executed / placements,
 # on the full-occupancy capture, profiles/eval_kernel_full_occupancy.md) and its DRAM bytes per full-generation launch
 # (ncu dram__bytes_read.sum + dram__bytes_write.sum, 1-pass capture of the full launch).
-LANE_INSTR_PER_PLACEMENT = 550
+LANE_INSTR_PER_PLACEMENT = 541
 DRAM_BYTES_PER_LAUNCH = 888_576
 
 

@@ -414,6 +414,37 @@ __device__ __forceinline__ uint64_t shfl64_up(uint64_t v) {
     return (uint64_t(__shfl_up_sync(FULL_MASK, uint32_t(v >> 32), 1)) << 32) | __shfl_up_sync(FULL_MASK, uint32_t(v), 1);
 }
 
+__device__ __forceinline__ uint64_t shfl64_xor(uint64_t v, int m) {
+    return (uint64_t(__shfl_xor_sync(FULL_MASK, uint32_t(v >> 32), m)) << 32) | __shfl_xor_sync(FULL_MASK, uint32_t(v), m);
+}
+
+// Bitonic sort of one key per lane into descending order (lane i = i-th largest).
+__device__ __forceinline__ uint64_t warp_sort_desc(uint64_t v, int lane) {
+#pragma unroll
+    for (int k = 2; k <= WARP; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            uint64_t const o = shfl64_xor(v, j);
+            bool const keep_max = ((lane & j) == 0) == ((lane & k) == 0);   // descending runs where lane & k == 0
+            v = keep_max ? (v > o ? v : o) : (v < o ? v : o);
+        }
+    }
+    return v;
+}
+
+// Bitonic merge of two descending 32-key lists (lane i = i-th largest) into the top kl keys.
+__device__ __forceinline__ uint64_t merge_topk(uint64_t a, uint64_t b, int kl, int lane) {
+    uint64_t const rb = shfl64(b, 31 - lane);                    // ascending
+    uint64_t c = a > rb ? a : rb;                                // bitonic, holds the 32 largest of both
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        uint64_t const o = shfl64_xor(c, j);
+        bool const lower = (lane & j) == 0;
+        c = lower ? (c > o ? c : o) : (c < o ? c : o);
+    }
+    return lane < kl ? c : 0ull;
+}
+
 // Fold one key per lane into the warp's sorted top-K list (lane i = i-th largest, 0 = empty;
 // `thr` caches list[k-1]): the keys above thr are inserted one at a time by ballot/shuffle. The
 // threshold is refreshed once per round, not after every insertion: a key that an earlier
@@ -463,37 +494,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
-}
-
-__device__ __forceinline__ uint64_t shfl64_xor(uint64_t v, int m) {
-    return (uint64_t(__shfl_xor_sync(FULL_MASK, uint32_t(v >> 32), m)) << 32) | __shfl_xor_sync(FULL_MASK, uint32_t(v), m);
-}
-
-// Bitonic sort of one key per lane into descending order (lane i = i-th largest).
-__device__ __forceinline__ uint64_t warp_sort_desc(uint64_t v, int lane) {
-#pragma unroll
-    for (int k = 2; k <= WARP; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            uint64_t const o = shfl64_xor(v, j);
-            bool const keep_max = ((lane & j) == 0) == ((lane & k) == 0);   // descending runs where lane & k == 0
-            v = keep_max ? (v > o ? v : o) : (v < o ? v : o);
-        }
-    }
-    return v;
-}
-
-// Bitonic merge of two descending 32-key lists (lane i = i-th largest) into the top kl keys.
-__device__ __forceinline__ uint64_t merge_topk(uint64_t a, uint64_t b, int kl, int lane) {
-    uint64_t const rb = shfl64(b, 31 - lane);                    // ascending
-    uint64_t c = a > rb ? a : rb;                                // bitonic, holds the 32 largest of both
-#pragma unroll
-    for (int j = 16; j > 0; j >>= 1) {
-        uint64_t const o = shfl64_xor(c, j);
-        bool const lower = (lane & j) == 0;
-        c = lower ? (c > o ? c : o) : (c < o ? c : o);
-    }
-    return lane < kl ? c : 0ull;
 }
 
 // ---------------------------------------------------------------- kernel ---
