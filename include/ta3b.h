@@ -196,6 +196,14 @@ int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out);
  * in ta3b_config) fixes the variant for every batch. */
 int ta3b_num_variants(void);
 int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm);
+/* Tail hand-off (on by default): a full batch on the default variant hands the
+ * games still playing when at most 4 per SM are left to the paired kernel, which
+ * finishes them two warps each (checkpointed at a move boundary; same results bit
+ * for bit). ta3b_set_tail_handoff(ctx, 0) keeps every game on one warp;
+ * ta3b_handoff_info reports how many games the context's last launch handed over
+ * (synchronises the context's stream). */
+int ta3b_set_tail_handoff(ta3b_ctx* ctx, int on);
+int ta3b_handoff_info(ta3b_ctx* ctx, uint32_t* games_out);
 int ta3b_variant_warps_per_game(int variant);
 int ta3b_select_variant(ta3b_ctx* ctx, int variant);
 

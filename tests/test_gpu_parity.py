@@ -78,6 +78,38 @@ def test_small_batches_run_on_the_paired_kernel(ev, ev_solo):
         assert out["trace"][i][:3 * nm].tobytes() == ref["trace"][i][:3 * nm].tobytes(), i
 
 
+def test_tail_handoff_is_bit_identical(ev):
+    """A full batch on the default variant hands the games still playing at the launch's tail to
+    the paired kernel (checkpointed at a move boundary); every output equals the launch that keeps
+    each game on one warp, traces included, and games really were handed over."""
+    from tetris_ai3_b200 import workload
+    b = workload.generation_batch(islands=4, pop=50, games=50, max_moves=300, seed=3)
+    w, seeds = b.weights, b.seeds[0]
+    ev.select_variant(7)
+    try:
+        ev.set_tail_handoff(True)
+        on = ev.eval_trace(w, w.shape[0], seeds, b.max_moves)
+        handed = ev.handoff_games()
+        ev.set_tail_handoff(False)
+        off = ev.eval_trace(w, w.shape[0], seeds, b.max_moves)
+        assert ev.handoff_games() == 0
+    finally:
+        ev.set_tail_handoff(True)
+    assert 0 < handed <= 4 * ev.launch_info()["sms"]
+    for k in ("score", "pieces", "lines", "evals", "moves", "board"):
+        assert on[k].tobytes() == off[k].tobytes(), k
+    for i, nm in enumerate(on["moves"]):
+        assert on["trace"][i][:3 * nm].tobytes() == off["trace"][i][:3 * nm].tobytes(), i
+    sc, pc, lc = ev.eval_islands(b.weights, b.seeds, b.max_moves)      # the island entry point hands over too
+    assert ev.handoff_games() > 0
+    ev.set_tail_handoff(False)
+    try:
+        s2, p2, l2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    finally:
+        ev.set_tail_handoff(True)
+    assert sc.tobytes() == s2.tobytes() and np.array_equal(pc, p2) and np.array_equal(lc, l2)
+
+
 def test_golden_games_single_warp_kernel(ev_solo, golden_games):
     """The golden batches are small, so a default context plays them on the paired kernel; the
     single-warp kernel plays them bit for bit too."""

@@ -38,7 +38,10 @@ constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
 // The work queue's scratch words: a 64-bit sim ticket (words 0-1) and the error status (word 2:
 // bit 0 = a search found no move although a root was legal, bit 1 = the time budget ran out).
 constexpr int kStatusWord = 2;
-constexpr size_t kScratchBytes = 16;
+// the tail hand-off (single-warp kernel -> paired kernel): warps that found no sim, the hand-off
+// flag, games checkpointed, and the paired kernel's ticket over the checkpoints
+constexpr int kDoneWord = 3, kHandoffWord = 4, kCkptCountWord = 5, kCkptTicketWord = 6;
+constexpr size_t kScratchBytes = 32;
 constexpr uint32_t kNoSim = 0xFFFFFFFFu;                 // never a sim index: sims <= 2^32 - 1
 constexpr uint64_t kMaxSims = 0xFFFFFFFFull;
 
@@ -568,14 +571,27 @@ struct Params {
     uint8_t* trace;
     uint32_t* n_moves;
     uint32_t* board_out;
-    uint32_t* scratch;                 // 16-byte aligned: [0..1] 64-bit sim ticket, [2] error status
+    uint32_t* scratch;                 // 16-byte aligned: [0..1] 64-bit sim ticket, [2] error status,
+                                       // [3..6] the tail hand-off's words
     unsigned long long* timing;        // optional: per sim [start, end] global timer (ns)
     unsigned long long* keys;          // tracing flavour: per move the final argmax's two largest keys
     unsigned long long budget_ns;      // 0, or the launch's time budget: past it warps stop and set status bit 2
     uint32_t num_games, models_per_island, max_moves, total_sims;
     uint32_t warps_active;             // 0, or the warps of each block that play (a batch smaller than
                                        // the grid's slots is spread over every SM); the rest take no sim
+    struct Checkpoint* ckpt;           // the tail hand-off's checkpoints (ckpt_cap of them)
+    uint32_t ckpt_cap;
+    uint32_t handoff_at;               // hand-off flavour: hand the games over when at most this many play
+    uint32_t resume;                   // paired kernel: play the checkpointed games instead of the sims
 };
+
+// A game handed from the single-warp kernel to the paired kernel at a move boundary.
+struct Checkpoint {
+    Engine eng;
+    Stats st;
+    uint32_t sim, moves, evals, pad;
+};
+static_assert(sizeof(Engine) % 4 == 0 && sizeof(Stats) % 4 == 0, "checkpoints are copied by words");
 
 struct Move {
     int orient, x, hold;
@@ -1027,6 +1043,36 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     return mv;
 }
 
+// Checkpoint the warp's game (engine, stats; its sim, moves and evaluation count parked in the
+// warp's pair_sim / pair_total / pair_cmd words) for the paired kernel. false when the array is full.
+__device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, Checkpoint* ckpt, uint32_t cap,
+                                             int lane) {
+    uint32_t idx = 0;
+    if (lane == 0) idx = atomicAdd(&scratch[kCkptCountWord], 1u);
+    idx = __shfl_sync(FULL_MASK, idx, 0);
+    if (idx >= cap) return false;
+    Checkpoint* const c = ckpt + idx;
+    uint32_t const* const e = reinterpret_cast<uint32_t const*>(&ws->eng);
+    uint32_t const* const t = reinterpret_cast<uint32_t const*>(&ws->st);
+    for (int i = lane; i < int(sizeof(Engine) / 4); i += WARP) reinterpret_cast<uint32_t*>(&c->eng)[i] = e[i];
+    for (int i = lane; i < int(sizeof(Stats) / 4); i += WARP) reinterpret_cast<uint32_t*>(&c->st)[i] = t[i];
+    if (lane == 0) {
+        c->sim = ws->pair_sim;
+        c->moves = ws->pair_total;
+        c->evals = ws->pair_cmd;
+    }
+    return true;
+}
+
+// The paired kernel's resume: the leader warp takes the checkpointed game's state.
+__device__ __noinline__ void load_checkpoint(WarpShared* ws, Checkpoint const* c, int lane) {
+    uint32_t* const e = reinterpret_cast<uint32_t*>(&ws->eng);
+    uint32_t* const t = reinterpret_cast<uint32_t*>(&ws->st);
+    for (int i = lane; i < int(sizeof(Engine) / 4); i += WARP) e[i] = reinterpret_cast<uint32_t const*>(&c->eng)[i];
+    for (int i = lane; i < int(sizeof(Stats) / 4); i += WARP) t[i] = reinterpret_cast<uint32_t const*>(&c->st)[i];
+    __syncwarp();
+}
+
 // NET: 0 = the v11 model; H = the widened 10 -> H -> H -> 1 network (64: 4,929 weights per
 // model, 32: 1,441) instead of v11.
 // BUDGET: the flavour that checks the launch's time budget after every move (a separate
@@ -1035,11 +1081,18 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
 // PAIR: two warps per game (v11 only, no budget, no key tracing): the even warp of each pair
 // takes the tickets, commits the moves and writes the results, the odd warp runs half of every
 // candidate pass (search_move's PAIR mode); results are the single-warp kernel's, bit for bit.
-template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false, bool PAIR = false>
+// With p.resume it plays the games a HANDOFF launch checkpointed.
+// HANDOFF: the launch's tail goes to the paired kernel. A warp that finds no sim left counts
+// itself done; when at most p.handoff_at warps still play, it raises the hand-off flag, and every
+// playing warp then checkpoints its game at its next move boundary (checked every 4th move) and
+// ends; the paired kernel, launched next on the same stream, finishes those games two warps each.
+template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false, bool PAIR = false,
+          bool HANDOFF = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;
     static_assert(!PAIR || (!WIDE && !BUDGET && !KEYS && WARPS % 2 == 0), "paired kernels: v11, whole pairs");
+    static_assert(!HANDOFF || (!WIDE && !BUDGET && !KEYS && !PAIR), "hand-off: the single-warp v11 kernel");
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
     for (int t = int(threadIdx.x); t < NPIECE * MP; t += WARPS * 32) {
@@ -1055,6 +1108,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         if (!partner) pair_bar_init(pr);
         pr[partner ? 1 : 0].pair_broken = 0;
     }
+    if (HANDOFF && lane == 0) ws.eng.over = 0;                 // (read after the game loop)
     __syncthreads();
     Luts const lut{s_lut.fast, s_lut.move};
     // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
@@ -1067,13 +1121,26 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     for (;;) {
         // a 64-bit ticket: every resident warp draws one past the last sim, which a 32-bit
         // counter could wrap near 2^32 sims; kNoSim (no sim index is that large) ends the warp
-        uint32_t sim = 0;
+        uint32_t sim = 0, ck = 0;
         if (!partner && lane == 0) {
-            // a warp beyond the block's playing warps takes no ticket (the batch is spread over the SMs)
             sim = kNoSim;
-            if (!p.warps_active || (threadIdx.x >> 5) < p.warps_active) {
+            if (PAIR && p.resume) {
+                // the checkpointed games, spread over the blocks
+                uint32_t n = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kCkptCountWord]);
+                n = n < p.ckpt_cap ? n : p.ckpt_cap;
+                if ((threadIdx.x >> 6) < (n + gridDim.x - 1) / gridDim.x) {
+                    ck = atomicAdd(&p.scratch[kCkptTicketWord], 1u);
+                    if (ck < n) sim = p.ckpt[ck].sim;
+                }
+            } else if (!p.warps_active || (threadIdx.x >> 5) < p.warps_active) {
+                // (a warp beyond the block's playing warps takes no ticket: the batch is spread over the SMs)
                 unsigned long long const t = atomicAdd(reinterpret_cast<unsigned long long*>(p.scratch), 1ull);
                 if (t < p.total_sims) sim = uint32_t(t);
+            }
+            if (HANDOFF && sim == kNoSim) {
+                uint32_t const total = gridDim.x * (p.warps_active ? p.warps_active : uint32_t(WARPS));
+                uint32_t const done = atomicAdd(&p.scratch[kDoneWord], 1u) + 1u;
+                if (total - done <= p.handoff_at) atomicExch(&p.scratch[kHandoffWord], 1u);
             }
         }
         if (PAIR) {                                                // the leader hands the sim to its partner
@@ -1088,7 +1155,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
         float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WideNet<HW>::STRIDE : NPARAMS);
-        if (p.timing && lane == 0) {
+        bool const resumed = PAIR && p.resume;
+        if (p.timing && lane == 0 && !resumed) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
             p.timing[2 * size_t(sim)] = t;
@@ -1099,8 +1167,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         if (!partner) {
             if (!WIDE)
                 for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
-            if (lane == 0) {
-                ws.wglobal = wsrc;
+            if (lane == 0) ws.wglobal = wsrc;
+            if (resumed) {
+                Checkpoint const* const c = p.ckpt + __shfl_sync(FULL_MASK, ck, 0);
+                load_checkpoint(&ws, c, lane);
+                moves = c->moves;
+                if (lane == 0) evals = c->evals;
+            } else if (lane == 0) {
                 engine_reset(ws.eng, seed);
                 ws.st = Stats{};
             }
@@ -1108,7 +1181,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         __syncwarp();
         // PAIR: the partner's one search_move call serves the whole game (it returns when the
         // leader ends the game), so both roles run the same copy of the search code
-        for (uint32_t mv_i = 0; partner || (mv_i < p.max_moves && !ws.eng.over); ++mv_i) {   // model_eval_host.cpp:39-50
+        while (partner || (moves < p.max_moves && !ws.eng.over)) {   // model_eval_host.cpp:39-50
             Move const mv = search_move<NET, KEYS, PAIR>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
             if (partner) break;
             if (PAIR && ws.pair_broken) break;
@@ -1133,6 +1206,15 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             ++moves;
             __syncwarp();
             if (ws.eng.over == 2) break;
+            if (HANDOFF && (moves & 3u) == 0 && moves < p.max_moves && !ws.eng.over) {
+                uint32_t f = 0;
+                if (lane == 0) f = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kHandoffWord]);
+                if (__shfl_sync(FULL_MASK, f, 0)) {
+                    if (lane == 0) ws.eng.over = 4;                  // to be handed over (below)
+                    __syncwarp();
+                    break;
+                }
+            }
             if (BUDGET) {                                          // over = 3: out of time, stop here
                 if (lane == 0) {
                     unsigned long long now;
@@ -1160,7 +1242,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
         if (PAIR) evals += pr[1].rec[0][66];
-        if (lane == 0) {
+        if (HANDOFF && lane == 0 && ws.eng.over == 4) {            // checkpointed after the game loop
+            ws.pair_sim = sim;
+            ws.pair_total = moves;
+            ws.pair_cmd = evals;
+        } else if (lane == 0) {
             p.score[sim] = final_score(ws.st);
             if (p.pieces) p.pieces[sim] = ws.st.pieces;
             if (p.lines) p.lines[sim] = ws.st.lines;
@@ -1176,6 +1262,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         }
         __syncwarp();
         if (BUDGET && ws.eng.over == 3) break;                   // out of time: take no further sim
+        if (HANDOFF && ws.eng.over == 4) break;                  // handed over: take no further sim
+    }
+    // the paired kernel finishes a handed-over game; at most handoff_at <= ckpt_cap games are
+    // still playing when the flag rises, so a full array is an error (the game's results stay unwritten)
+    if (HANDOFF && ws.eng.over == 4) {
+        __syncwarp();
+        if (!save_checkpoint(&ws, p.scratch, p.ckpt, p.ckpt_cap, lane) && lane == 0)
+            atomicOr(&p.scratch[kStatusWord], 8u);
     }
 }
 
@@ -1256,6 +1350,9 @@ Variant const kVariants[] = {
     // most 4 games per SM run on it by default
     {eval_kernel<8, 1, 0, false, false, true>, 8, 1, true},
 };
+// the default variant's hand-off flavour: its launch's tail (at most 4 games per SM) goes to the
+// paired kernel
+Variant const kHandoffVariant = {eval_kernel<16, 1, 0, false, false, false, true>, 16, 1};
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // the networks a launch can run: v11, or the widened 10 -> H -> H -> 1 for H = 64 or 32
 enum NetKind { NET_V11 = 0, NET_W64 = 1, NET_W32 = 2, NUM_NETS = 3 };
@@ -1315,6 +1412,10 @@ struct ta3b_ctx {
     uint32_t keys_grid[NUM_NETS] = {0, 0, 0};    // key-tracing flavours (by NetKind), set up on first use
     bool auto_small = true;                      // small v11 batches run the paired kernel (until a variant is selected)
     uint32_t small_grid = 0;                     // its grid, set up on first use
+    bool handoff = true;                         // the default variant hands its launch's tail to the paired kernel
+    uint32_t handoff_grid = 0;                   // the hand-off flavour's grid, set up on first use
+    Checkpoint* d_ckpt = nullptr;                // the hand-off's checkpoints: one per paired-kernel game slot
+    uint32_t ckpt_cap = 0;
     uint64_t* d_keys = nullptr;                  // per move the two largest final keys (tracing)
     size_t cap_keys = 0;
     uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
@@ -1462,7 +1563,26 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     Params p2 = prm;
     p2.warps_active = spread ? (sims + grid - 1) / grid * (warps / games) : 0u;
     p2.budget_ns = ctx->budget_ns;
-    v->fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
+    // the default variant on a full batch: its launch's tail (at most one paired-kernel slot's worth
+    // of games still playing) is checkpointed and finished by the paired kernel, two warps a game
+    bool const handoff = ctx->handoff && ctx->d_ckpt && v == &kVariants[kDefaultVariant] && !spread;
+    if (handoff) {
+        if (!ctx->handoff_grid)
+            if (int rc = setup_kernel(ctx, kHandoffVariant, NET_V11, ctx->handoff_grid, "hand-off kernel")) return rc;
+        if (!ctx->small_grid)
+            if (int rc = setup_kernel(ctx, small, NET_V11, ctx->small_grid, "paired kernel")) return rc;
+        p2.ckpt = ctx->d_ckpt;
+        p2.ckpt_cap = ctx->ckpt_cap;
+        p2.handoff_at = ctx->ckpt_cap < ctx->small_grid * small.games() ? ctx->ckpt_cap : ctx->small_grid * small.games();
+        kHandoffVariant.fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
+        TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
+        Params p3 = p2;
+        p3.resume = 1;
+        p3.warps_active = 0;
+        small.fn<<<ctx->small_grid, small.warps * 32, small.warps * warp_bytes(NET_V11), st>>>(p3);
+    } else {
+        v->fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
+    }
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     ctx->last_grid = grid;
     ctx->last_warps = warps;
@@ -1636,11 +1756,13 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
     if (cudaSetDevice(c.device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_scratch, kScratchBytes) != cudaSuccess ||
-        cudaMemset(ctx->d_scratch, 0, kScratchBytes) != cudaSuccess) {
+        cudaMemset(ctx->d_scratch, 0, kScratchBytes) != cudaSuccess ||
+        cudaMalloc(&ctx->d_ckpt, size_t(ctx->sms) * kVariants[kSmallVariant].games() * sizeof(Checkpoint)) != cudaSuccess) {
         g_create_error = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());
         ta3b_destroy(ctx);
         return nullptr;
     }
+    ctx->ckpt_cap = ctx->sms * kVariants[kSmallVariant].games();
     int v = kDefaultVariant;
     if (c.warps_per_block || c.blocks_per_sm) {
         v = -1;
@@ -1670,7 +1792,7 @@ void ta3b_destroy(ta3b_ctx* ctx) {
     cudaSetDevice(ctx->device);
     void* bufs[] = {ctx->d_w, ctx->d_seeds, ctx->d_score, ctx->d_pieces, ctx->d_lines, ctx->d_evals,
                     ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing, ctx->d_wpad,
-                    ctx->d_keys};
+                    ctx->d_keys, ctx->d_ckpt};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1789,6 +1911,22 @@ int ta3b_core_selftest(uint32_t const* recs, uint32_t num_recs, uint32_t const* 
         g_create_error = std::string("core selftest: ") + cudaGetErrorString(e);
         return TA3B_ERR_CUDA;
     }
+    return TA3B_OK;
+}
+
+int ta3b_set_tail_handoff(ta3b_ctx* ctx, int on) {
+    if (!ctx) return TA3B_ERR_ARG;
+    ctx->handoff = on != 0;
+    return TA3B_OK;
+}
+
+int ta3b_handoff_info(ta3b_ctx* ctx, uint32_t* games_out) {
+    if (!ctx || !games_out) return TA3B_ERR_ARG;
+    uint32_t n = 0;
+    TA3B_CUDA(ctx, cudaMemcpyAsync(&n, ctx->d_scratch + kCkptCountWord, sizeof n, cudaMemcpyDeviceToHost, ctx->stream),
+              "read hand-off count");
+    TA3B_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "read hand-off count");
+    *games_out = n < ctx->ckpt_cap ? n : ctx->ckpt_cap;
     return TA3B_OK;
 }
 

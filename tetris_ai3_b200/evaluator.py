@@ -32,7 +32,7 @@ _lib = None
 
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
            "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
-           "ta3b_variant_warps_per_game",
+           "ta3b_variant_warps_per_game", "ta3b_set_tail_handoff", "ta3b_handoff_info",
            "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc", "ta3b_set_time_budget",
            "ta3b_device_status", "ta3b_noalloc_status"]
 
@@ -70,6 +70,8 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_num_variants.argtypes = []
     lib.ta3b_variant_info.argtypes = [C.c_int, vp, vp]
     lib.ta3b_variant_warps_per_game.argtypes = [C.c_int]
+    lib.ta3b_set_tail_handoff.argtypes = [vp, C.c_int]
+    lib.ta3b_handoff_info.argtypes = [vp, vp]
     lib.ta3b_select_variant.argtypes = [vp, C.c_int]
     lib.ta3b_set_time_budget.argtypes = [vp, C.c_double]
     lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
@@ -261,6 +263,16 @@ class ModelEvaluator:
 
     def select_variant(self, variant: int):
         self._check(self._lib.ta3b_select_variant(self._ctx, variant))
+
+    def set_tail_handoff(self, on: bool):
+        """Hand a full batch's tail to the paired kernel (default on); off keeps every game on one warp."""
+        self._check(self._lib.ta3b_set_tail_handoff(self._ctx, int(bool(on))))
+
+    def handoff_games(self) -> int:
+        """How many games the last launch handed to the paired kernel."""
+        n = C.c_uint32()
+        self._check(self._lib.ta3b_handoff_info(self._ctx, C.byref(n)))
+        return n.value
 
     @staticmethod
     def variants():
