@@ -1043,10 +1043,11 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     return mv;
 }
 
-// Checkpoint the warp's game (engine, stats; its sim, moves and evaluation count parked in the
-// warp's pair_sim / pair_total / pair_cmd words) for the paired kernel. false when the array is full.
+// Checkpoint the warp's game for the paired kernel: engine and stats, the sim (parked in the warp's
+// pair_sim word), its moves (= pieces placed: the game goes on, so no move failed) and evaluation
+// count (the provisional result the warp wrote). false when the array is full.
 __device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, Checkpoint* ckpt, uint32_t cap,
-                                             int lane) {
+                                             uint32_t const* evals, int lane) {
     uint32_t idx = 0;
     if (lane == 0) idx = atomicAdd(&scratch[kCkptCountWord], 1u);
     idx = __shfl_sync(FULL_MASK, idx, 0);
@@ -1056,10 +1057,13 @@ __device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, 
     uint32_t const* const t = reinterpret_cast<uint32_t const*>(&ws->st);
     for (int i = lane; i < int(sizeof(Engine) / 4); i += WARP) reinterpret_cast<uint32_t*>(&c->eng)[i] = e[i];
     for (int i = lane; i < int(sizeof(Stats) / 4); i += WARP) reinterpret_cast<uint32_t*>(&c->st)[i] = t[i];
+    __syncwarp();
     if (lane == 0) {
-        c->sim = ws->pair_sim;
-        c->moves = ws->pair_total;
-        c->evals = ws->pair_cmd;
+        uint32_t const sim = ws->pair_sim;
+        c->eng.over = 0;                                // (ws->eng.over holds the hand-off marker)
+        c->sim = sim;
+        c->moves = ws->st.pieces;                       // every committed move placed one piece
+        c->evals = evals ? evals[sim] : 0u;             // the provisional result the warp just wrote
     }
     return true;
 }
@@ -1167,7 +1171,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         if (!partner) {
             if (!WIDE)
                 for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
-            if (lane == 0) ws.wglobal = wsrc;
+            if (lane == 0) {
+                ws.wglobal = wsrc;
+                if (HANDOFF) ws.pair_sim = sim;                    // (read by the hand-off's checkpoint)
+            }
             if (resumed) {
                 Checkpoint const* const c = p.ckpt + __shfl_sync(FULL_MASK, ck, 0);
                 load_checkpoint(&ws, c, lane);
@@ -1210,7 +1217,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 uint32_t f = 0;
                 if (lane == 0) f = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kHandoffWord]);
                 if (__shfl_sync(FULL_MASK, f, 0)) {
-                    if (lane == 0) ws.eng.over = 4;                  // to be handed over (below)
+                    if (lane == 0) ws.eng.over = 4;                  // handed over after the game loop
                     __syncwarp();
                     break;
                 }
@@ -1242,11 +1249,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
         if (PAIR) evals += pr[1].rec[0][66];
-        if (HANDOFF && lane == 0 && ws.eng.over == 4) {            // checkpointed after the game loop
-            ws.pair_sim = sim;
-            ws.pair_total = moves;
-            ws.pair_cmd = evals;
-        } else if (lane == 0) {
+        if (lane == 0) {
             p.score[sim] = final_score(ws.st);
             if (p.pieces) p.pieces[sim] = ws.st.pieces;
             if (p.lines) p.lines[sim] = ws.st.lines;
@@ -1262,13 +1265,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         }
         __syncwarp();
         if (BUDGET && ws.eng.over == 3) break;                   // out of time: take no further sim
-        if (HANDOFF && ws.eng.over == 4) break;                  // handed over: take no further sim
     }
-    // the paired kernel finishes a handed-over game; at most handoff_at <= ckpt_cap games are
-    // still playing when the flag rises, so a full array is an error (the game's results stay unwritten)
+    // The paired kernel finishes a handed-over game (over = 4; the game's results written above are
+    // provisional: the paired kernel overwrites them). At most handoff_at <= ckpt_cap games are
+    // still playing when the flag rises, so a full array is an error.
     if (HANDOFF && ws.eng.over == 4) {
         __syncwarp();
-        if (!save_checkpoint(&ws, p.scratch, p.ckpt, p.ckpt_cap, lane) && lane == 0)
+        if (!save_checkpoint(&ws, p.scratch, p.ckpt, p.ckpt_cap, p.evals, lane) && lane == 0)
             atomicOr(&p.scratch[kStatusWord], 8u);
     }
 }
