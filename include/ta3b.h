@@ -218,10 +218,13 @@ int ta3b_select_variant(ta3b_ctx* ctx, int variant);
 int ta3b_core_selftest(const uint32_t* recs, uint32_t num_recs, const uint32_t* cand, uint32_t n, const float* w97,
                        float* fast_v, int* fast_st, float* full_v, int* full_legal, float* dbg32);
 
-/* Launch shape of the context's most recent kernel launch (before the first
- * one: the selected variant's full grid): grid blocks, warps per block, and the
- * device's SM count. For tooling and the autotuner. */
-int ta3b_launch_info(const ta3b_ctx* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms);
+/* Launch shape of the context's most recent evaluation (before the first one:
+ * the selected variant's full grid): grid blocks and warps per block of its
+ * first kernel, the device's SM count, and how many kernels the evaluation
+ * launched (2 with the tail hand-off's paired kernel, else 1; 0 before the
+ * first). Any output may be NULL. For tooling and the autotuner. */
+int ta3b_launch_info(const ta3b_ctx* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms,
+                     uint32_t* kernels);
 
 #ifdef __cplusplus
 }

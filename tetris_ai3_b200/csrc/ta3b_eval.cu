@@ -1422,6 +1422,7 @@ struct ta3b_ctx {
     uint64_t* d_keys = nullptr;                  // per move the two largest final keys (tracing)
     size_t cap_keys = 0;
     uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
+    uint32_t last_kernels = 0;                // and how many kernels it launched
     std::string err;
 };
 
@@ -1589,6 +1590,7 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     ctx->last_grid = grid;
     ctx->last_warps = warps;
+    ctx->last_kernels = handoff ? 2u : 1u;
     return TA3B_OK;
 }
 
@@ -1959,11 +1961,13 @@ int ta3b_select_variant(ta3b_ctx* ctx, int variant) {
     return select_variant(ctx, variant);
 }
 
-int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms) {
+int ta3b_launch_info(ta3b_ctx const* ctx, uint32_t* grid, uint32_t* warps_per_block, uint32_t* sms,
+                     uint32_t* kernels) {
     if (!ctx) return TA3B_ERR_ARG;
     if (grid) *grid = ctx->last_grid ? ctx->last_grid : ctx->grid;
     if (warps_per_block) *warps_per_block = ctx->last_grid ? ctx->last_warps : ctx->warps_per_block;
     if (sms) *sms = ctx->sms;
+    if (kernels) *kernels = ctx->last_kernels;
     return TA3B_OK;
 }
 

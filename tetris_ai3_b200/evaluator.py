@@ -66,7 +66,7 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_eval_trace.argtypes = [vp, vp, u32, u32, vp, u32, u32, vp, vp, vp, vp, vp, vp, vp, vp]
     lib.ta3b_eval_timed.argtypes = [vp, vp, u32, u32, u32, vp, u32, u32, vp, vp, vp, vp]
     lib.ta3b_simulate_seeds.argtypes = [u64, u32, vp]
-    lib.ta3b_launch_info.argtypes = [vp, vp, vp, vp]
+    lib.ta3b_launch_info.argtypes = [vp, vp, vp, vp, vp]
     lib.ta3b_num_variants.argtypes = []
     lib.ta3b_variant_info.argtypes = [C.c_int, vp, vp]
     lib.ta3b_variant_warps_per_game.argtypes = [C.c_int]
@@ -314,8 +314,9 @@ class ModelEvaluator:
 
     def launch_info(self):
         g, w, s = C.c_uint32(), C.c_uint32(), C.c_uint32()
-        self._check(self._lib.ta3b_launch_info(self._ctx, C.byref(g), C.byref(w), C.byref(s)))
-        return {"grid": g.value, "warps_per_block": w.value, "sms": s.value}
+        k = C.c_uint32()
+        self._check(self._lib.ta3b_launch_info(self._ctx, C.byref(g), C.byref(w), C.byref(s), C.byref(k)))
+        return {"grid": g.value, "warps_per_block": w.value, "sms": s.value, "kernels": k.value}
 
 
 def simulate(evaluator: ModelEvaluator, model_weights, num_models: int, games: int, seed: int,
