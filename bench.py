@@ -58,11 +58,11 @@ METRIC_WIDE32 = ("beam placements/s on 1 B200 (widened 10-32-32-1 evaluator: 8 i
                  "= 80k sims, cap 2000)")
 METRICS = {"wide": METRIC_WIDE, "wide32": METRIC_WIDE32, "stress": METRIC_STRESS}
 HIDDEN = {"wide": 64, "wide32": 32}           # the widened models' hidden width
-# What this kernel executes per placement (ncu thread_inst_executed / placements,
-# on the full-occupancy capture, profiles/eval_kernel_full_occupancy.md) and its DRAM bytes per full-generation launch
-# (ncu dram__bytes_read.sum + dram__bytes_write.sum, 1-pass capture of the full launch).
+# What the single-warp kernel executes per placement (ncu thread_inst_executed / placements, on a
+# full-occupancy capture) and the DRAM bytes of one full-generation evaluation (ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of its two launches, 1-pass capture).
 LANE_INSTR_PER_PLACEMENT = 541
-DRAM_BYTES_PER_LAUNCH = 888_576
+DRAM_BYTES_PER_LAUNCH = 1_181_184
 
 
 from tetris_ai3_b200.dist import rank_env as _dist_env, rank_seed, reduce_timing  # noqa: E402
