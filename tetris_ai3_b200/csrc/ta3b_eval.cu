@@ -283,6 +283,17 @@ struct WideIn {
 template <int H>
 constexpr int kWideHbFloats = H * WARP;                // per warp: H units x 32 lanes (8 KB for 64)
 
+// four units' sums += x * q: the products as two packed multiplies (each half rounded like the
+// scalar multiply), the additions scalar, so that no multiply is fused into an add
+__device__ __forceinline__ void wide_fold4(float* a, float2 x, float4 q) {
+    float2 const p01 = f2_mul(x, make_float2(q.x, q.y));
+    float2 const p23 = f2_mul(x, make_float2(q.z, q.w));
+    a[0] = f_add(a[0], p01.x);
+    a[1] = f_add(a[1], p01.y);
+    a[2] = f_add(a[2], p23.x);
+    a[3] = f_add(a[3], p23.y);
+}
+
 template <int H>
 __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w, float* __restrict__ hb, int lane) {
     static_assert(H >= 4 && H <= 64 && H % 4 == 0, "the hidden-unit masks hold 64 units");
@@ -303,14 +314,11 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
     for (int i = 0; i < NIN; ++i) {
         if (!((inz >> i) & 1u)) continue;
         float4 const* wr = reinterpret_cast<float4 const*>(w + D::W1T + i * H);
-        float const x = in.v[i];
+        float2 const x = make_float2(in.v[i], in.v[i]);
 #pragma unroll
         for (int o = 0; o < H; o += 4) {
             float4 const q = __ldg(wr + o / 4);
-            a[o] = f_add(a[o], f_mul(x, q.x));
-            a[o + 1] = f_add(a[o + 1], f_mul(x, q.y));
-            a[o + 2] = f_add(a[o + 2], f_mul(x, q.z));
-            a[o + 3] = f_add(a[o + 3], f_mul(x, q.w));
+            wide_fold4(a + o, x, q);
         }
     }
     // ReLU into the buffer; nz = the units that are non-zero in some lane
@@ -345,15 +353,12 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
     while (m) {
         int const i = __ffsll(static_cast<long long>(m)) - 1;
         m &= m - 1;
-        float const x = hs[i * WARP];
+        float2 const x = make_float2(hs[i * WARP], hs[i * WARP]);
         float4 const* wr = reinterpret_cast<float4 const*>(w + D::W2T + i * H);
 #pragma unroll
         for (int o = 0; o < H; o += 4) {
             float4 const q = __ldg(wr + o / 4);
-            a[o] = f_add(a[o], f_mul(x, q.x));
-            a[o + 1] = f_add(a[o + 1], f_mul(x, q.y));
-            a[o + 2] = f_add(a[o + 2], f_mul(x, q.z));
-            a[o + 3] = f_add(a[o + 3], f_mul(x, q.w));
+            wide_fold4(a + o, x, q);
         }
     }
     // layer 3: every term, ascending
@@ -361,10 +366,12 @@ __device__ __noinline__ float wide_value(WideIn in, float const* __restrict__ w,
 #pragma unroll
     for (int o = 0; o < H; o += 4) {
         float4 const q = __ldg(reinterpret_cast<float4 const*>(w + D::W3 + o));
-        out = f_add(out, f_mul(relu(a[o]), q.x));
-        out = f_add(out, f_mul(relu(a[o + 1]), q.y));
-        out = f_add(out, f_mul(relu(a[o + 2]), q.z));
-        out = f_add(out, f_mul(relu(a[o + 3]), q.w));
+        float2 const t01 = f2_mul(make_float2(relu(a[o]), relu(a[o + 1])), make_float2(q.x, q.y));
+        float2 const t23 = f2_mul(make_float2(relu(a[o + 2]), relu(a[o + 3])), make_float2(q.z, q.w));
+        out = f_add(out, t01.x);
+        out = f_add(out, t01.y);
+        out = f_add(out, t23.x);
+        out = f_add(out, t23.y);
     }
     return out;
 }
