@@ -313,6 +313,21 @@ def test_generation_graph_replays_match_direct_calls(ev):
         assert (ec > 0).all()
 
 
+def test_generation_graph_with_tail_handoff(ev):
+    """A full generation captured as a CUDA graph runs both kernels of the tail hand-off (the
+    single-warp kernel and the paired kernel) and replays the direct call's results."""
+    from tetris_ai3_b200 import workload
+    from tetris_ai3_b200.evaluator import GenerationGraph
+    g = GenerationGraph(ev, models=200, islands=4, games=50, max_moves=120)
+    for seed in (41, 42):
+        b = workload.generation_batch(islands=4, pop=50, games=50, max_moves=120, seed=seed)
+        sc, pc, lc, ec = g.run(b.weights, b.seeds)
+        assert ev.handoff_games() > 0
+        s2, p2, l2 = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+        assert ev.launch_info()["kernels"] == 2
+        assert sc.tobytes() == s2.tobytes() and np.array_equal(pc, p2) and np.array_equal(lc, l2)
+
+
 def test_time_budget_stops_the_launch_and_keeps_the_context(ev):
     """A budget far below the batch's run time ends the launch early with
     TA3B_ERR_TIMEOUT (no fault); without a budget the same context then scores
