@@ -57,10 +57,11 @@ def test_variants_enumerate(lib):
     v = ModelEvaluator.variants()
     assert len(v) == lib.ta3b_num_variants() >= 2
     solo = [x for x in v if x["warps_per_game"] == 1]
-    pair = [x for x in v if x["warps_per_game"] == 2]
-    assert len(solo) + len(pair) == len(v) and pair
+    teams = [x for x in v if x["warps_per_game"] > 1]
+    assert len(solo) + len(teams) == len(v) and teams
     assert {x["warps_per_block"] for x in solo} == {2, 4, 8, 10, 16, 20}
-    assert all(x["warps_per_block"] % 2 == 0 for x in pair)
+    assert {x["warps_per_game"] for x in teams} == {2, 4, 8}
+    assert all(x["warps_per_block"] % x["warps_per_game"] == 0 for x in teams)
     assert lib.ta3b_variant_warps_per_game(-1) == -1 and lib.ta3b_variant_warps_per_game(len(v)) == -1
 
 

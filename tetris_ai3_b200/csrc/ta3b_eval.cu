@@ -484,21 +484,23 @@ __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
     return v;
 }
 
-// ----------------------------------------------------------------- pairs ---
-// Paired kernels play every game with two warps of a block: the even warp (the leader) owns
-// the game and runs everything but the candidate passes alone; in each stage the two warps
-// take alternate 32-candidate rounds (leader rounds 0, 2, 4, ..., partner 1, 3, 5, ...), each
-// keeps its own top-K list, argmax, legality bits and evaluation count, and the leader merges
-// the partner's (keys are unique within a stage, so the result is the single-warp one). A game
-// therefore runs faster while the issue work per move stays the same, which shortens a launch's
-// tail of long games. The two warps synchronise through a counter barrier in shared memory
-// whose wait gives up after kPairWaitNs (no legitimate wait comes near it): the warp sets
-// status bit STATUS_PAIR and leaves, and the call reports TA3B_ERR_DEVICE.
+// ----------------------------------------------------------------- teams ---
+// Team kernels play every game with TEAM (2, 4 or 8) consecutive warps of a block: the first
+// warp (the leader) owns the game and runs everything but the candidate passes alone; in each
+// stage the team's warps take the 32-candidate rounds in turn (warp r of the team takes rounds
+// r, r + TEAM, r + 2 TEAM, ...), each keeps its own top-K list, argmax, legality bits and
+// evaluation count, and the leader merges the partners' (keys are unique within a stage, so the
+// result is the single-warp one). A game therefore runs faster while the issue work per move stays
+// the same, which shortens a launch's tail of long games. A team synchronises through an mbarrier
+// whose waits give up after kPairWaitNs (no legitimate wait comes near it): the warp sets status
+// bit STATUS_PAIR and leaves, and the call reports TA3B_ERR_DEVICE.
 constexpr uint32_t PAIR_GAME_END = 0xFFFFFFFFu;
 constexpr unsigned long long kPairWaitNs = 1000000000ull;    // 1 s
 constexpr uint32_t STATUS_PAIR = 4u;
-// the partner's stage results, in its own (unused) record area
-constexpr int X_BEST = 32, X_BITS = 33, X_EVALS = 34;
+// a partner's stage results, in its own (otherwise unused) record area: its list (or per-lane
+// argmax) in words 0-63, its legality bits in words X_LO / X_HI; its game's evaluation count in
+// X_EVALS
+constexpr int X_LO = 64, X_HI = 65, X_EVALS = 66;
 
 __device__ __forceinline__ unsigned long long global_ns() {
     unsigned long long t;
@@ -518,27 +520,28 @@ struct alignas(16) WarpShared {
     uint32_t seg_info[64];             // rec (6) | rank k << 8 | piece << 16 | held-is-I << 20 | child << 21
     uint32_t defer[64];                // queued (segment << 8 | placement) for the full path
     alignas(8) uint64_t kbuf[WARP];    // a level's keys above the top-K threshold, not yet merged
-    // paired kernels (two warps per game; the game lives in the even warp's area)
-    alignas(8) unsigned long long pair_bar;   // game area: the pair's barrier (an mbarrier of 2 arrivals)
+    // team kernels (TEAM warps per game; the game lives in the leader's area)
+    alignas(8) unsigned long long pair_bar;   // game area: the team's barrier (an mbarrier of TEAM arrivals)
     uint32_t pair_cmd;                 // game area: the stage to run next, or PAIR_GAME_END
     uint32_t pair_total;               // game area: that stage's candidate count
-    uint32_t pair_sim;                 // game area: the sim the pair plays (kNoSim: none left)
-    uint32_t pair_broken;              // this warp: a pair wait ran out
+    uint32_t pair_sim;                 // game area: the sim the team plays (kNoSim: none left)
+    uint32_t pair_broken;              // this warp: a team wait ran out
     uint32_t pad_pair_[2];
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte alignment");
 
-// The pair barrier (pr[0] the leader's area, pr[1] the partner's): an mbarrier in the game area
-// that completes a phase when both warps' lane 0 have arrived. Arrival releases and the wait
-// acquires, so the warps' shared-memory writes before the barrier are visible to the mate after
+// The team barrier (pr[0] the leader's area, pr[r] warp r's): an mbarrier in the game area that
+// completes a phase when every team warp's lane 0 has arrived. Arrival releases and the wait
+// acquires, so the warps' shared-memory writes before the barrier are visible to the others after
 // it. The wait polls mbarrier.try_wait (which suspends the thread in hardware between polls) and
 // gives up after kPairWaitNs: false = it ran out (status bit set, this warp's pair_broken set).
-__device__ __forceinline__ void pair_bar_init(WarpShared* pr) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(uint32_t(__cvta_generic_to_shared(&pr[0].pair_bar)))
+__device__ __forceinline__ void pair_bar_init(WarpShared* pr, uint32_t team) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
+                 ::"r"(uint32_t(__cvta_generic_to_shared(&pr[0].pair_bar))), "r"(team)
                  : "memory");
 }
 
-__device__ __forceinline__ bool pair_sync(WarpShared* pr, bool partner, uint32_t* status, int lane) {
+__device__ __forceinline__ bool pair_sync(WarpShared* pr, int rank, uint32_t* status, int lane) {
     int ok = 1;
     __syncwarp();
     if (lane == 0) {
@@ -557,7 +560,7 @@ __device__ __forceinline__ bool pair_sync(WarpShared* pr, bool partner, uint32_t
             if (polls == 0) t0 = global_ns();
             else if ((polls & 15u) == 0 && global_ns() - t0 > kPairWaitNs) {
                 atomicOr(status, STATUS_PAIR);
-                pr[partner ? 1 : 0].pair_broken = 1u;
+                pr[rank].pair_broken = 1u;
                 ok = 0;
                 break;
             }
@@ -679,7 +682,7 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality. ws is the game's area, own the warp's own (its queue of deferred
 // candidates and its key buffer; the same area except in paired kernels).
-// PAIR: this warp takes every other 32-candidate round, starting at candidate `first`.
+// TEAM > 1: this warp takes every TEAM-th 32-candidate round, starting at candidate `first`.
 //
 // The top-kl list (lane i = i-th largest, 0 = empty; thr = list[kl-1]): keys are unique per level
 // (the low word encodes the slot), so the kept set equals beam.hpp:244-265's "max score, lowest
@@ -690,7 +693,7 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // thr is below the final list[kl-1] too. The lazy merge shortens a warp's critical path (15 %
 // per move for a warp alone on its scheduler) but executes more instructions, which costs 3-5 %
 // at 16 warps per SM, where the single-warp kernels run.
-template <int NET, bool KEYS, bool PAIR = false>
+template <int NET, bool KEYS, int TEAM = 1>
 __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, Luts lut, FastW const& fw, float* hb,
                                                bool leaf, uint32_t total, int kl, int lane, uint32_t& evals,
                                                uint32_t first = 0) {
@@ -698,6 +701,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
     uint32_t* const dq = own.defer;
     uint64_t* const kb = own.kbuf;
+    constexpr bool PAIR = TEAM > 1;
     constexpr bool LAZY = PAIR;
     LevelAcc acc{0, 0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
@@ -783,7 +787,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
             uint32_t const dm = __ballot_sync(FULL_MASK, def);
             if (def) dq[queued + __popc(dm & ((1u << lane) - 1u))] = (sg << 8) | idx;
             queued += __popc(dm);
-            c0 += PAIR ? 2u * WARP : uint32_t(WARP);
+            c0 += uint32_t(TEAM * WARP);
         }
         if (leaf) {
             if (KEYS) top2_insert(acc.best, acc.best2, key);
@@ -874,15 +878,17 @@ __device__ __forceinline__ void root_record(WarpShared* ws, Luts lut, int lane) 
 }
 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game.
-// PAIR: ws is the pair's game (the leader's area, the partner's follows it). The leader runs the
-// search and posts each stage; the partner stays in here for the whole game, runs the stages it
-// is posted (its half of each candidate pass) and returns when the leader posts PAIR_GAME_END.
-template <int NET, bool KEYS, bool PAIR = false>
+// TEAM > 1: ws is the team's game (the leader's area, the partners' follow it). The leader runs
+// the search and posts each stage; a partner stays in here for the whole game, runs the stages it
+// is posted (its share of each candidate pass) and returns when the leader posts PAIR_GAME_END.
+template <int NET, bool KEYS, int TEAM = 1>
 __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
     constexpr bool WIDE = NET != 0;
-    static_assert(!PAIR || (!WIDE && !KEYS), "paired kernels run the v11 model without key tracing");
-    bool const partner = PAIR && (threadIdx.x & 32u) != 0;
+    constexpr bool PAIR = TEAM > 1;
+    static_assert(!PAIR || (!WIDE && !KEYS), "team kernels run the v11 model without key tracing");
+    int const rank = PAIR ? int((threadIdx.x >> 5) & uint32_t(TEAM - 1)) : 0;
+    bool const partner = rank != 0;
     WarpShared* const pr = &ws;
     Move mv{0, 0, 0, true, 0, 0};
     if (!partner && ws.eng.over) return mv;
@@ -910,7 +916,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         // ---- segments of this stage
         uint32_t total;
         if (partner) {                         // the stage the leader posts, or the end of the game
-            if (!pair_sync(pr, true, status, lane)) return mv;
+            if (!pair_sync(pr, rank, status, lane)) return mv;
             uint32_t const cmd = ws.pair_cmd;
             if (cmd == PAIR_GAME_END) return mv;
             stage = int(cmd);
@@ -941,34 +947,36 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
                 ws.pair_cmd = uint32_t(stage);
                 ws.pair_total = total;
             }
-            if (!pair_sync(pr, false, status, lane)) return mv;
+            if (!pair_sync(pr, 0, status, lane)) return mv;
         }
         bool const leaf = stage == DEPTH - 1;
         int const kl = stage == 0 ? K0 : (stage == 1 ? K1 : K2);
         // ---- every candidate of the stage
-        LevelAcc a = level_pass<NET, KEYS, PAIR>(ws, pr[partner ? 1 : 0], lut, fw, hb, leaf, total, kl, lane,
-                                                 evals, partner ? uint32_t(WARP) : 0u);
+        LevelAcc a = level_pass<NET, KEYS, TEAM>(ws, pr[rank], lut, fw, hb, leaf, total, kl, lane, evals,
+                                                 uint32_t(rank * WARP));
         if (PAIR) {
-            // the partner's results go through its own record area, which it never uses otherwise:
-            // its list (or per-lane argmax) in words 0-63, its legality bits in words 64-65
-            uint32_t* const x = pr[1].rec[0];
-            uint64_t* const xk = reinterpret_cast<uint64_t*>(x);
+            // a partner's results go through its own record area, which it never uses otherwise
             if (partner) {
-                xk[lane] = leaf ? a.best : a.list;
+                uint32_t* const x = pr[rank].rec[0];
+                reinterpret_cast<uint64_t*>(x)[lane] = leaf ? a.best : a.list;
                 uint32_t const lo = __reduce_or_sync(FULL_MASK, a.lo), hi = __reduce_or_sync(FULL_MASK, a.hi);
                 if (lane == 0) {
-                    x[64] = lo;
-                    x[65] = hi;
+                    x[X_LO] = lo;
+                    x[X_HI] = hi;
                 }
-                if (!pair_sync(pr, true, status, lane)) return mv;
+                if (!pair_sync(pr, rank, status, lane)) return mv;
                 continue;
             }
-            if (!pair_sync(pr, false, status, lane)) return mv;
-            uint64_t const b = xk[lane];
-            if (leaf) a.best = b > a.best ? b : a.best;
-            else a.list = merge_topk(a.list, b, kl, lane);
-            a.lo |= x[64];
-            a.hi |= x[65];
+            if (!pair_sync(pr, 0, status, lane)) return mv;
+#pragma unroll 1
+            for (int m = 1; m < TEAM; ++m) {
+                uint32_t const* const x = pr[m].rec[0];
+                uint64_t const b = reinterpret_cast<uint64_t const*>(x)[lane];
+                if (leaf) a.best = b > a.best ? b : a.best;
+                else a.list = merge_topk(a.list, b, kl, lane);
+                a.lo |= x[X_LO];
+                a.hi |= x[X_HI];
+            }
         }
         if (stage == 0) {
             // ---- seed the frontier with the selected roots (beam.hpp:307-329): lane k = rank k
@@ -1039,8 +1047,8 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
     // ---- decode the winning key back to its root move (beam.hpp:450-470)
     uint32_t const order = ORDER_SPAN - uint32_t(best);
     uint32_t const leaf_rank = __shfl_sync(FULL_MASK, frank, int((order / (2 * MP)) & 31u));
-    uint32_t const rank = order >= uint32_t(LEAF_ORDERS) ? order - LEAF_ORDERS : leaf_rank;
-    uint32_t const rs = __shfl_sync(FULL_MASK, root_slot, int(rank & 31u));
+    uint32_t const root_rank = order >= uint32_t(LEAF_ORDERS) ? order - LEAF_ORDERS : leaf_rank;
+    uint32_t const rs = __shfl_sync(FULL_MASK, root_slot, int(root_rank & 31u));
     uint32_t const g = rs / MP;
     uint32_t const pa = lut.move[g ? p1 : p0][rs % MP];
     mv.orient = int((pa >> 20) & 3u);
@@ -1089,20 +1097,22 @@ __device__ __noinline__ void load_checkpoint(WarpShared* ws, Checkpoint const* c
 // BUDGET: the flavour that checks the launch's time budget after every move (a separate
 // instantiation: the check's registers would otherwise cost the ordinary kernels spills).
 // KEYS: the tracing flavour that also records each move's two largest final keys (p.keys).
-// PAIR: two warps per game (v11 only, no budget, no key tracing): the even warp of each pair
-// takes the tickets, commits the moves and writes the results, the odd warp runs half of every
-// candidate pass (search_move's PAIR mode); results are the single-warp kernel's, bit for bit.
-// With p.resume it plays the games a HANDOFF launch checkpointed.
-// HANDOFF: the launch's tail goes to the paired kernel. A warp that finds no sim left counts
-// itself done; when at most p.handoff_at warps still play, it raises the hand-off flag, and every
-// playing warp then checkpoints its game at its next move boundary (checked every 4th move) and
-// ends; the paired kernel, launched next on the same stream, finishes those games two warps each.
-template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false, bool PAIR = false,
+// TEAM: warps per game; TEAM > 1 (v11 only, no budget, no key tracing): the team's first warp
+// takes the tickets, commits the moves and writes the results, the others run their share of
+// every candidate pass (search_move's team mode); results are the single-warp kernel's, bit for
+// bit. With p.resume it plays the games a HANDOFF launch checkpointed.
+// HANDOFF: the launch's tail goes to a team kernel. A warp that finds no sim left counts itself
+// done; when at most p.handoff_at warps still play, it raises the hand-off flag, and every playing
+// warp then checkpoints its game at its next move boundary (checked every 4th move) and ends; the
+// team kernel, launched next on the same stream, finishes those games.
+template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false, int TEAM = 1,
           bool HANDOFF = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;
-    static_assert(!PAIR || (!WIDE && !BUDGET && !KEYS && WARPS % 2 == 0), "paired kernels: v11, whole pairs");
+    constexpr bool PAIR = TEAM > 1;
+    static_assert(TEAM == 1 || TEAM == 2 || TEAM == 4 || TEAM == 8, "teams of 1, 2, 4 or 8 warps");
+    static_assert(!PAIR || (!WIDE && !BUDGET && !KEYS && WARPS % TEAM == 0), "team kernels: v11, whole teams");
     static_assert(!HANDOFF || (!WIDE && !BUDGET && !KEYS && !PAIR), "hand-off: the single-warp v11 kernel");
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
@@ -1111,13 +1121,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         s_lut.move[t / MP][t % MP] = g_lut.move[t / MP][t % MP];
     }
     int const lane = int(threadIdx.x & 31u);
-    bool const partner = PAIR && (threadIdx.x & 32u) != 0;
-    // PAIR: pr[0] is the pair's game (the leader's area), pr[1] the partner's area
-    WarpShared* const pr = reinterpret_cast<WarpShared*>(dyn_smem) + (PAIR ? (threadIdx.x >> 5) & ~1u : threadIdx.x >> 5);
+    int const rank = PAIR ? int((threadIdx.x >> 5) & uint32_t(TEAM - 1)) : 0;
+    bool const partner = rank != 0;
+    // TEAM > 1: pr[0] is the team's game (the leader's area), pr[r] warp r's area
+    WarpShared* const pr = reinterpret_cast<WarpShared*>(dyn_smem) + ((threadIdx.x >> 5) & ~uint32_t(TEAM - 1));
     WarpShared& ws = pr[0];
     if (PAIR && lane == 0) {
-        if (!partner) pair_bar_init(pr);
-        pr[partner ? 1 : 0].pair_broken = 0;
+        if (!partner) pair_bar_init(pr, uint32_t(TEAM));
+        pr[rank].pair_broken = 0;
     }
     if (HANDOFF && lane == 0) ws.eng.over = 0;                 // (read after the game loop)
     __syncthreads();
@@ -1139,7 +1150,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 // the checkpointed games, spread over the blocks
                 uint32_t n = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kCkptCountWord]);
                 n = n < p.ckpt_cap ? n : p.ckpt_cap;
-                if ((threadIdx.x >> 6) < (n + gridDim.x - 1) / gridDim.x) {
+                if ((threadIdx.x >> 5) / uint32_t(TEAM) < (n + gridDim.x - 1) / gridDim.x) {
                     ck = atomicAdd(&p.scratch[kCkptTicketWord], 1u);
                     if (ck < n) sim = p.ckpt[ck].sim;
                 }
@@ -1154,9 +1165,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (total - done <= p.handoff_at) atomicExch(&p.scratch[kHandoffWord], 1u);
             }
         }
-        if (PAIR) {                                                // the leader hands the sim to its partner
+        if (PAIR) {                                                // the leader hands the sim to its partners
             if (!partner && lane == 0) ws.pair_sim = sim;
-            if (!pair_sync(pr, partner, &p.scratch[kStatusWord], lane)) break;
+            if (!pair_sync(pr, rank, &p.scratch[kStatusWord], lane)) break;
             sim = __shfl_sync(FULL_MASK, ws.pair_sim, 0);
         } else {
             sim = __shfl_sync(FULL_MASK, sim, 0);
@@ -1196,7 +1207,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         // PAIR: the partner's one search_move call serves the whole game (it returns when the
         // leader ends the game), so both roles run the same copy of the search code
         while (partner || (moves < p.max_moves && !ws.eng.over)) {   // model_eval_host.cpp:39-50
-            Move const mv = search_move<NET, KEYS, PAIR>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
+            Move const mv = search_move<NET, KEYS, TEAM>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
             if (partner) break;
             if (PAIR && ws.pair_broken) break;
             if (KEYS && lane == 0 && p.keys) {
@@ -1242,20 +1253,22 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (ws.eng.over == 3) break;
             }
         }
-        if (PAIR) {                           // the leader ends the partner's game and takes its count
-            if (pr[partner ? 1 : 0].pair_broken) break;
+        if (PAIR) {                           // the leader ends the partners' game and takes their counts
+            if (pr[rank].pair_broken) break;
             if (!partner) {
                 if (lane == 0) ws.pair_cmd = PAIR_GAME_END;
-                if (!pair_sync(pr, false, &p.scratch[kStatusWord], lane)) break;
+                if (!pair_sync(pr, 0, &p.scratch[kStatusWord], lane)) break;
             } else {
                 uint32_t const own = __reduce_add_sync(FULL_MASK, evals);
-                if (lane == 0) pr[1].rec[0][66] = own;
+                if (lane == 0) pr[rank].rec[0][X_EVALS] = own;
             }
-            if (!pair_sync(pr, partner, &p.scratch[kStatusWord], lane)) break;
+            if (!pair_sync(pr, rank, &p.scratch[kStatusWord], lane)) break;
             if (partner) continue;
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
-        if (PAIR) evals += pr[1].rec[0][66];
+        if (PAIR)
+#pragma unroll 1
+            for (int m = 1; m < TEAM; ++m) evals += pr[m].rec[0][X_EVALS];
         if (lane == 0) {
             p.score[sim] = final_score(ws.st);
             if (p.pieces) p.pieces[sim] = ws.st.pieces;
@@ -1346,8 +1359,8 @@ using KernelFn = void (*)(Params);
 struct Variant {
     KernelFn fn;
     uint32_t warps, min_blocks;
-    bool pair = false;                 // two warps per game (eval_pair_kernel)
-    uint32_t games() const { return pair ? warps / 2 : warps; }
+    uint32_t team = 1;                 // warps per game
+    uint32_t games() const { return warps / team; }
 };
 Variant const kVariants[] = {
     {eval_kernel<4, 3>, 4, 3}, {eval_kernel<4, 4>, 4, 4}, {eval_kernel<4, 5>, 4, 5}, {eval_kernel<4, 6>, 4, 6},
@@ -1358,11 +1371,13 @@ Variant const kVariants[] = {
     {eval_kernel<10, 2>, 10, 2}, {eval_kernel<20, 1>, 20, 1},
     // two warps per game, 4 games per block (one block per SM, no register cap): batches of at
     // most 4 games per SM run on it by default
-    {eval_kernel<8, 1, 0, false, false, true>, 8, 1, true},
+    {eval_kernel<8, 1, 0, false, false, 2>, 8, 1, 2},
+    // four and eight warps per game (2 and 1 games per block), for A/B against the paired kernel
+    {eval_kernel<8, 1, 0, false, false, 4>, 8, 1, 4}, {eval_kernel<8, 1, 0, false, false, 8>, 8, 1, 8},
 };
 // the default variant's hand-off flavour: its launch's tail (at most 4 games per SM) goes to the
 // paired kernel
-Variant const kHandoffVariant = {eval_kernel<16, 1, 0, false, false, false, true>, 16, 1};
+Variant const kHandoffVariant = {eval_kernel<16, 1, 0, false, false, 1, true>, 16, 1};
 constexpr int kNumVariants = int(sizeof(kVariants) / sizeof(kVariants[0]));
 // the networks a launch can run: v11, or the widened 10 -> H -> H -> 1 for H = 64 or 32
 enum NetKind { NET_V11 = 0, NET_W64 = 1, NET_W32 = 2, NUM_NETS = 3 };
@@ -1779,7 +1794,7 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
     if (c.warps_per_block || c.blocks_per_sm) {
         v = -1;
         for (int i = 0; i < kNumVariants; ++i)
-            if (!kVariants[i].pair && (!c.warps_per_block || kVariants[i].warps == c.warps_per_block) &&
+            if (kVariants[i].team == 1 && (!c.warps_per_block || kVariants[i].warps == c.warps_per_block) &&
                 (!c.blocks_per_sm || kVariants[i].min_blocks == c.blocks_per_sm)) {
                 v = i;
                 break;
@@ -1946,7 +1961,7 @@ int ta3b_num_variants(void) { return kNumVariants; }
 
 int ta3b_variant_warps_per_game(int variant) {
     if (variant < 0 || variant >= kNumVariants) return -1;
-    return kVariants[variant].pair ? 2 : 1;
+    return int(kVariants[variant].team);
 }
 
 int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_blocks_per_sm) {
