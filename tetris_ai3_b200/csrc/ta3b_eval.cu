@@ -1372,8 +1372,9 @@ Variant const kVariants[] = {
     // two warps per game, 4 games per block (one block per SM, no register cap): batches of at
     // most 4 games per SM run on it by default
     {eval_kernel<8, 1, 0, false, false, 2>, 8, 1, 2},
-    // four and eight warps per game (2 and 1 games per block), for A/B against the paired kernel
-    {eval_kernel<8, 1, 0, false, false, 4>, 8, 1, 4}, {eval_kernel<8, 1, 0, false, false, 8>, 8, 1, 8},
+    // four warps per game (2 games per block): 55 vs 65 us per move at one game per SM, 63 vs 67 at
+    // two (eight warps per game measured 69 us: the per-warp top-K and the merges stop the gain)
+    {eval_kernel<8, 1, 0, false, false, 4>, 8, 1, 4},
 };
 // the default variant's hand-off flavour: its launch's tail (at most 4 games per SM) goes to the
 // paired kernel
