@@ -190,8 +190,9 @@ int ta3b_simulate_seeds(uint64_t seed, uint32_t games, uint64_t* seeds_out);
  * bit), -1 for a variant out of range. ta3b_config's warps_per_block /
  * blocks_per_sm select among the single-warp variants only.
  * Launch shape: a context created with the tuned default runs a batch of at most
- * 4 games per SM (v11 network, no time budget, no key tracing) on the paired
- * kernel and every other batch on the default variant; a batch smaller than one
+ * 2 games per SM (v11 network, no time budget, no key tracing) on teams of four
+ * warps, one of at most 4 games per SM on the paired kernel, and every other
+ * batch on the default variant; a batch smaller than one
  * block per SM can hold is spread over all SMs. ta3b_select_variant (or a shape
  * in ta3b_config) fixes the variant for every batch. */
 int ta3b_num_variants(void);

@@ -62,9 +62,10 @@ def ev_solo():
     e.close()
 
 
-def test_small_batches_run_on_the_paired_kernel(ev, ev_solo):
-    """A default context plays a batch of at most 4 games per SM with two warps per game, spread one
-    block per SM; a selected variant is kept for every batch. Same bits, same evaluation counts."""
+def test_small_batches_run_on_team_kernels(ev, ev_solo):
+    """A default context plays a batch of at most 2 games per SM with four warps per game (at most
+    4: two), spread one block per SM; a selected variant is kept for every batch. Same bits, same
+    evaluation counts."""
     from tetris_ai3_b200 import workload
     b = workload.generation_batch(islands=2, pop=5, games=12, max_moves=300, seed=21)
     out = ev.eval_trace(b.weights[:10], 10, b.seeds[0], b.max_moves)

@@ -1397,6 +1397,7 @@ Variant const kKeysNet[NUM_NETS] = {{eval_kernel<4, 3, 0, false, true>, 4, 3},
                                     {eval_kernel<4, 3, 32, false, true>, 4, 3}};
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kSmallVariant = 10;  // the paired kernel: the default for batches of at most 4 games per SM
+constexpr int kTinyVariant = 11;   // teams of four: the default for batches of at most 2 games per SM
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
 } // namespace
@@ -1438,6 +1439,7 @@ struct ta3b_ctx {
     uint32_t keys_grid[NUM_NETS] = {0, 0, 0};    // key-tracing flavours (by NetKind), set up on first use
     bool auto_small = true;                      // small v11 batches run the paired kernel (until a variant is selected)
     uint32_t small_grid = 0;                     // its grid, set up on first use
+    uint32_t tiny_grid = 0;                      // the teams-of-four kernel's grid (the smallest batches)
     bool handoff = true;                         // the default variant hands its launch's tail to the paired kernel
     uint32_t handoff_grid = 0;                   // the hand-off flavour's grid, set up on first use
     Checkpoint* d_ckpt = nullptr;                // the hand-off's checkpoints: one per paired-kernel game slot
@@ -1564,22 +1566,27 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     TA3B_CUDA(ctx, cudaMemsetAsync(prm.scratch, 0, kScratchBytes, st), "reset work queue");
     // with a time budget the budget-checking flavour runs, with key tracing the tracing flavour
     // (which runs without the budget); each has its own fixed launch shape
-    // a v11 batch of at most 4 games per SM runs on the paired kernel (two warps per game), whose
-    // moves take 0.69x the single-warp kernel's time at that load, unless a variant was selected
+    // unless a variant was selected, a v11 batch of at most 4 games per SM runs on the paired kernel
+    // (two warps per game), whose moves take 0.62x the single-warp kernel's time at that load, and
+    // one of at most 2 games per SM on teams of four warps (0.53x)
     Variant const& small = kVariants[kSmallVariant];
-    bool const use_small = ctx->auto_small && ni == NET_V11 && !keys && !budget &&
-                           prm.total_sims <= ctx->sms * small.games();
+    Variant const& tiny = kVariants[kTinyVariant];
+    bool const auto_small = ctx->auto_small && ni == NET_V11 && !keys && !budget;
+    bool const use_tiny = auto_small && prm.total_sims <= ctx->sms * tiny.games();
+    bool const use_small = auto_small && !use_tiny && prm.total_sims <= ctx->sms * small.games();
     if (use_small && !ctx->small_grid)
         if (int rc = setup_kernel(ctx, small, NET_V11, ctx->small_grid, "paired kernel")) return rc;
+    if (use_tiny && !ctx->tiny_grid)
+        if (int rc = setup_kernel(ctx, tiny, NET_V11, ctx->tiny_grid, "teams-of-four kernel")) return rc;
     Variant const* const v = keys     ? &kKeysNet[ni]
                              : budget ? &kBudgetNet[ni]
                              : ni != NET_V11 ? &kWideNet[ni]
-                             : use_small ? &small : &kVariants[ctx->variant];
+                             : use_tiny ? &tiny : use_small ? &small : &kVariants[ctx->variant];
     uint32_t const warps = v->warps, games = v->games();
     uint32_t const max_grid = keys     ? ctx->keys_grid[ni]
                               : budget ? ctx->budget_grid[ni]
                               : ni != NET_V11 ? ctx->net_grid[ni]
-                              : use_small ? ctx->small_grid : ctx->grid;
+                              : use_tiny ? ctx->tiny_grid : use_small ? ctx->small_grid : ctx->grid;
     // a batch that one block per SM can hold is spread over every SM, one block each (a game runs
     // faster on an SM it shares with fewer others), rather than packed into the fewest blocks
     uint32_t const sims = prm.total_sims;
