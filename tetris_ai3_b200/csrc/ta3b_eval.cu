@@ -492,11 +492,11 @@ __device__ __forceinline__ uint64_t warp_max64(uint64_t v) {
 // evaluation count, and the leader merges the partners' (keys are unique within a stage, so the
 // result is the single-warp one). A game therefore runs faster while the issue work per move stays
 // the same, which shortens a launch's tail of long games. A team synchronises through an mbarrier
-// whose waits give up after kPairWaitNs (no legitimate wait comes near it): the warp sets status
-// bit STATUS_PAIR and leaves, and the call reports TA3B_ERR_DEVICE.
-constexpr uint32_t PAIR_GAME_END = 0xFFFFFFFFu;
-constexpr unsigned long long kPairWaitNs = 1000000000ull;    // 1 s
-constexpr uint32_t STATUS_PAIR = 4u;
+// whose waits give up after kTeamWaitNs (no legitimate wait comes near it): the warp sets status
+// bit STATUS_TEAM and leaves, and the call reports TA3B_ERR_DEVICE.
+constexpr uint32_t TEAM_GAME_END = 0xFFFFFFFFu;
+constexpr unsigned long long kTeamWaitNs = 1000000000ull;    // 1 s
+constexpr uint32_t STATUS_TEAM = 4u;
 // a partner's stage results, in its own (otherwise unused) record area: its list (or per-lane
 // argmax) in words 0-63, its legality bits in words X_LO / X_HI; its game's evaluation count in
 // X_EVALS
@@ -521,12 +521,12 @@ struct alignas(16) WarpShared {
     uint32_t defer[64];                // queued (segment << 8 | placement) for the full path
     alignas(8) uint64_t kbuf[WARP];    // a level's keys above the top-K threshold, not yet merged
     // team kernels (TEAM warps per game; the game lives in the leader's area)
-    alignas(8) unsigned long long pair_bar;   // game area: the team's barrier (an mbarrier of TEAM arrivals)
-    uint32_t pair_cmd;                 // game area: the stage to run next, or PAIR_GAME_END
-    uint32_t pair_total;               // game area: that stage's candidate count
-    uint32_t pair_sim;                 // game area: the sim the team plays (kNoSim: none left)
-    uint32_t pair_broken;              // this warp: a team wait ran out
-    uint32_t pad_pair_[2];
+    alignas(8) unsigned long long team_bar;   // game area: the team's barrier (an mbarrier of TEAM arrivals)
+    uint32_t team_cmd;                 // game area: the stage to run next, or TEAM_GAME_END
+    uint32_t team_total;               // game area: that stage's candidate count
+    uint32_t team_sim;                 // game area: the sim the team plays (kNoSim: none left)
+    uint32_t team_broken;              // this warp: a team wait ran out
+    uint32_t pad_team_[2];
 };
 static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte alignment");
 
@@ -534,18 +534,18 @@ static_assert(sizeof(WarpShared) % 16 == 0, "warp blocks must keep 16-byte align
 // completes a phase when every team warp's lane 0 has arrived. Arrival releases and the wait
 // acquires, so the warps' shared-memory writes before the barrier are visible to the others after
 // it. The wait polls mbarrier.try_wait (which suspends the thread in hardware between polls) and
-// gives up after kPairWaitNs: false = it ran out (status bit set, this warp's pair_broken set).
-__device__ __forceinline__ void pair_bar_init(WarpShared* pr, uint32_t team) {
+// gives up after kTeamWaitNs: false = it ran out (status bit set, this warp's team_broken set).
+__device__ __forceinline__ void team_bar_init(WarpShared* pr, uint32_t team) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;"
-                 ::"r"(uint32_t(__cvta_generic_to_shared(&pr[0].pair_bar))), "r"(team)
+                 ::"r"(uint32_t(__cvta_generic_to_shared(&pr[0].team_bar))), "r"(team)
                  : "memory");
 }
 
-__device__ __forceinline__ bool pair_sync(WarpShared* pr, int rank, uint32_t* status, int lane) {
+__device__ __forceinline__ bool team_sync(WarpShared* pr, int rank, uint32_t* status, int lane) {
     int ok = 1;
     __syncwarp();
     if (lane == 0) {
-        uint32_t const bar = uint32_t(__cvta_generic_to_shared(&pr[0].pair_bar));
+        uint32_t const bar = uint32_t(__cvta_generic_to_shared(&pr[0].team_bar));
         unsigned long long state;
         asm volatile("mbarrier.arrive.shared::cta.b64 %0, [%1];" : "=l"(state) : "r"(bar) : "memory");
         unsigned long long t0 = 0;
@@ -558,9 +558,9 @@ __device__ __forceinline__ bool pair_sync(WarpShared* pr, int rank, uint32_t* st
                 : "memory");
             if (done) break;
             if (polls == 0) t0 = global_ns();
-            else if ((polls & 15u) == 0 && global_ns() - t0 > kPairWaitNs) {
-                atomicOr(status, STATUS_PAIR);
-                pr[rank].pair_broken = 1u;
+            else if ((polls & 15u) == 0 && global_ns() - t0 > kTeamWaitNs) {
+                atomicOr(status, STATUS_TEAM);
+                pr[rank].team_broken = 1u;
                 ok = 0;
                 break;
             }
@@ -681,13 +681,13 @@ __device__ __noinline__ bool full_inputs_wide(WarpShared* ws, Luts lut, uint32_t
 // for the full path (evaluated in compacted 32-lane batches). leaf: fold into
 // the argmax key and per-list legality; otherwise into the top-kl list and
 // per-parent legality. ws is the game's area, own the warp's own (its queue of deferred
-// candidates and its key buffer; the same area except in paired kernels).
+// candidates and its key buffer; the same area except in team kernels).
 // TEAM > 1: this warp takes every TEAM-th 32-candidate round, starting at candidate `first`.
 //
 // The top-kl list (lane i = i-th largest, 0 = empty; thr = list[kl-1]): keys are unique per level
 // (the low word encodes the slot), so the kept set equals beam.hpp:244-265's "max score, lowest
 // slot on ties" whatever the order keys arrive in. The single-warp kernels insert each key above
-// thr at once (topk_fold). The paired kernels keep the list lazily: keys above thr go to the
+// thr at once (topk_fold). The team kernels keep the list lazily: keys above thr go to the
 // warp's key buffer, and when a round's keys would overflow it (or the level ends) the buffer is
 // sorted across the lanes and merged into the list, which raises thr; a key at or below a stale
 // thr is below the final list[kl-1] too. The lazy merge shortens a warp's critical path (15 %
@@ -701,8 +701,8 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
     constexpr int HW = WIDE ? NET : 64;     // the widened network's width (unused for v11)
     uint32_t* const dq = own.defer;
     uint64_t* const kb = own.kbuf;
-    constexpr bool PAIR = TEAM > 1;
-    constexpr bool LAZY = PAIR;
+    constexpr bool TEAMED = TEAM > 1;
+    constexpr bool LAZY = TEAMED;
     LevelAcc acc{0, 0, 0, 0, 0, 0};
     auto consume = [&](uint64_t key, uint32_t seg, uint32_t info) {
         if (key) {
@@ -721,7 +721,7 @@ __device__ __forceinline__ LevelAcc level_pass(WarpShared& ws, WarpShared& own, 
     uint32_t queued = 0;          // < 32 at the start of every fast round: the queue holds 64
     uint32_t kcnt = 0;            // keys in the key buffer (non-leaf levels)
     int seg = 0;
-    uint32_t c0 = PAIR ? first : 0u;
+    uint32_t c0 = TEAMED ? first : 0u;
     for (;;) {
         bool const more = c0 < total;
         // the level's candidates are done; a non-leaf level takes one more turn to merge its buffer
@@ -880,14 +880,14 @@ __device__ __forceinline__ void root_record(WarpShared* ws, Luts lut, int lane) 
 // search_move_beam (beam.hpp:484-570) for the warp's committed game.
 // TEAM > 1: ws is the team's game (the leader's area, the partners' follow it). The leader runs
 // the search and posts each stage; a partner stays in here for the whole game, runs the stages it
-// is posted (its share of each candidate pass) and returns when the leader posts PAIR_GAME_END.
+// is posted (its share of each candidate pass) and returns when the leader posts TEAM_GAME_END.
 template <int NET, bool KEYS, int TEAM = 1>
 __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW const& fw, float* hb, int lane, uint32_t& evals,
                                             uint32_t* status) {
     constexpr bool WIDE = NET != 0;
-    constexpr bool PAIR = TEAM > 1;
-    static_assert(!PAIR || (!WIDE && !KEYS), "team kernels run the v11 model without key tracing");
-    int const rank = PAIR ? int((threadIdx.x >> 5) & uint32_t(TEAM - 1)) : 0;
+    constexpr bool TEAMED = TEAM > 1;
+    static_assert(!TEAMED || (!WIDE && !KEYS), "team kernels run the v11 model without key tracing");
+    int const rank = TEAMED ? int((threadIdx.x >> 5) & uint32_t(TEAM - 1)) : 0;
     bool const partner = rank != 0;
     WarpShared* const pr = &ws;
     Move mv{0, 0, 0, true, 0, 0};
@@ -916,11 +916,11 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         // ---- segments of this stage
         uint32_t total;
         if (partner) {                         // the stage the leader posts, or the end of the game
-            if (!pair_sync(pr, rank, status, lane)) return mv;
-            uint32_t const cmd = ws.pair_cmd;
-            if (cmd == PAIR_GAME_END) return mv;
+            if (!team_sync(pr, rank, status, lane)) return mv;
+            uint32_t const cmd = ws.team_cmd;
+            if (cmd == TEAM_GAME_END) return mv;
             stage = int(cmd);
-            total = ws.pair_total;
+            total = ws.team_total;
         } else if (stage == DEPTH) {
             break;
         } else if (stage == 0) {               // two root groups over the committed board (beam.hpp:283-301)
@@ -942,19 +942,19 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         } else {
             total = build_segments(ws, slot_piece, tree, stage, fnode, kept, lane);
         }
-        if (PAIR && !partner) {                // post the stage
+        if (TEAMED && !partner) {                // post the stage
             if (lane == 0) {
-                ws.pair_cmd = uint32_t(stage);
-                ws.pair_total = total;
+                ws.team_cmd = uint32_t(stage);
+                ws.team_total = total;
             }
-            if (!pair_sync(pr, 0, status, lane)) return mv;
+            if (!team_sync(pr, 0, status, lane)) return mv;
         }
         bool const leaf = stage == DEPTH - 1;
         int const kl = stage == 0 ? K0 : (stage == 1 ? K1 : K2);
         // ---- every candidate of the stage
         LevelAcc a = level_pass<NET, KEYS, TEAM>(ws, pr[rank], lut, fw, hb, leaf, total, kl, lane, evals,
                                                  uint32_t(rank * WARP));
-        if (PAIR) {
+        if (TEAMED) {
             // a partner's results go through its own record area, which it never uses otherwise
             if (partner) {
                 uint32_t* const x = pr[rank].rec[0];
@@ -964,10 +964,10 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
                     x[X_LO] = lo;
                     x[X_HI] = hi;
                 }
-                if (!pair_sync(pr, rank, status, lane)) return mv;
+                if (!team_sync(pr, rank, status, lane)) return mv;
                 continue;
             }
-            if (!pair_sync(pr, 0, status, lane)) return mv;
+            if (!team_sync(pr, 0, status, lane)) return mv;
 #pragma unroll 1
             for (int m = 1; m < TEAM; ++m) {
                 uint32_t const* const x = pr[m].rec[0];
@@ -1059,7 +1059,7 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
 }
 
 // Checkpoint the warp's game for the paired kernel: engine and stats, the sim (parked in the warp's
-// pair_sim word), its moves (= pieces placed: the game goes on, so no move failed) and evaluation
+// team_sim word), its moves (= pieces placed: the game goes on, so no move failed) and evaluation
 // count (the provisional result the warp wrote). false when the array is full.
 __device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, Checkpoint* ckpt, uint32_t cap,
                                              uint32_t const* evals, int lane) {
@@ -1074,7 +1074,7 @@ __device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, 
     for (int i = lane; i < int(sizeof(Stats) / 4); i += WARP) reinterpret_cast<uint32_t*>(&c->st)[i] = t[i];
     __syncwarp();
     if (lane == 0) {
-        uint32_t const sim = ws->pair_sim;
+        uint32_t const sim = ws->team_sim;
         c->eng.over = 0;                                // (ws->eng.over holds the hand-off marker)
         c->sim = sim;
         c->moves = ws->st.pieces;                       // every committed move placed one piece
@@ -1110,10 +1110,10 @@ template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = fal
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     constexpr bool WIDE = NET != 0;
     constexpr int HW = WIDE ? NET : 64;
-    constexpr bool PAIR = TEAM > 1;
+    constexpr bool TEAMED = TEAM > 1;
     static_assert(TEAM == 1 || TEAM == 2 || TEAM == 4 || TEAM == 8, "teams of 1, 2, 4 or 8 warps");
-    static_assert(!PAIR || (!WIDE && !BUDGET && !KEYS && WARPS % TEAM == 0), "team kernels: v11, whole teams");
-    static_assert(!HANDOFF || (!WIDE && !BUDGET && !KEYS && !PAIR), "hand-off: the single-warp v11 kernel");
+    static_assert(!TEAMED || (!WIDE && !BUDGET && !KEYS && WARPS % TEAM == 0), "team kernels: v11, whole teams");
+    static_assert(!HANDOFF || (!WIDE && !BUDGET && !KEYS && !TEAMED), "hand-off: the single-warp v11 kernel");
     extern __shared__ __align__(16) unsigned char dyn_smem[];    // WARPS x WarpShared
     __shared__ LutTables s_lut;
     for (int t = int(threadIdx.x); t < NPIECE * MP; t += WARPS * 32) {
@@ -1121,14 +1121,14 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         s_lut.move[t / MP][t % MP] = g_lut.move[t / MP][t % MP];
     }
     int const lane = int(threadIdx.x & 31u);
-    int const rank = PAIR ? int((threadIdx.x >> 5) & uint32_t(TEAM - 1)) : 0;
+    int const rank = TEAMED ? int((threadIdx.x >> 5) & uint32_t(TEAM - 1)) : 0;
     bool const partner = rank != 0;
     // TEAM > 1: pr[0] is the team's game (the leader's area), pr[r] warp r's area
     WarpShared* const pr = reinterpret_cast<WarpShared*>(dyn_smem) + ((threadIdx.x >> 5) & ~uint32_t(TEAM - 1));
     WarpShared& ws = pr[0];
-    if (PAIR && lane == 0) {
-        if (!partner) pair_bar_init(pr, uint32_t(TEAM));
-        pr[rank].pair_broken = 0;
+    if (TEAMED && lane == 0) {
+        if (!partner) team_bar_init(pr, uint32_t(TEAM));
+        pr[rank].team_broken = 0;
     }
     if (HANDOFF && lane == 0) ws.eng.over = 0;                 // (read after the game loop)
     __syncthreads();
@@ -1146,7 +1146,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t sim = 0, ck = 0;
         if (!partner && lane == 0) {
             sim = kNoSim;
-            if (PAIR && p.resume) {
+            if (TEAMED && p.resume) {
                 // the checkpointed games, spread over the blocks
                 uint32_t n = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kCkptCountWord]);
                 n = n < p.ckpt_cap ? n : p.ckpt_cap;
@@ -1165,10 +1165,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (total - done <= p.handoff_at) atomicExch(&p.scratch[kHandoffWord], 1u);
             }
         }
-        if (PAIR) {                                                // the leader hands the sim to its partners
-            if (!partner && lane == 0) ws.pair_sim = sim;
-            if (!pair_sync(pr, rank, &p.scratch[kStatusWord], lane)) break;
-            sim = __shfl_sync(FULL_MASK, ws.pair_sim, 0);
+        if (TEAMED) {                                                // the leader hands the sim to its partners
+            if (!partner && lane == 0) ws.team_sim = sim;
+            if (!team_sync(pr, rank, &p.scratch[kStatusWord], lane)) break;
+            sim = __shfl_sync(FULL_MASK, ws.team_sim, 0);
         } else {
             sim = __shfl_sync(FULL_MASK, sim, 0);
         }
@@ -1177,7 +1177,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
         float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WideNet<HW>::STRIDE : NPARAMS);
-        bool const resumed = PAIR && p.resume;
+        bool const resumed = TEAMED && p.resume;
         if (p.timing && lane == 0 && !resumed) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -1191,7 +1191,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 for (int i = lane; i < NPARAMS; i += WARP) ws.wfull[i] = __ldg(wsrc + i);
             if (lane == 0) {
                 ws.wglobal = wsrc;
-                if (HANDOFF) ws.pair_sim = sim;                    // (read by the hand-off's checkpoint)
+                if (HANDOFF) ws.team_sim = sim;                    // (read by the hand-off's checkpoint)
             }
             if (resumed) {
                 Checkpoint const* const c = p.ckpt + __shfl_sync(FULL_MASK, ck, 0);
@@ -1204,12 +1204,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             }
         }
         __syncwarp();
-        // PAIR: the partner's one search_move call serves the whole game (it returns when the
+        // team kernels: a partner's one search_move call serves the whole game (it returns when the
         // leader ends the game), so both roles run the same copy of the search code
         while (partner || (moves < p.max_moves && !ws.eng.over)) {   // model_eval_host.cpp:39-50
             Move const mv = search_move<NET, KEYS, TEAM>(ws, lut, fw, hb, lane, evals, &p.scratch[kStatusWord]);
             if (partner) break;
-            if (PAIR && ws.pair_broken) break;
+            if (TEAMED && ws.team_broken) break;
             if (KEYS && lane == 0 && p.keys) {
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2] = mv.key1;
                 p.keys[(size_t(sim) * p.max_moves + moves) * 2 + 1] = mv.key2;
@@ -1253,20 +1253,20 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (ws.eng.over == 3) break;
             }
         }
-        if (PAIR) {                           // the leader ends the partners' game and takes their counts
-            if (pr[rank].pair_broken) break;
+        if (TEAMED) {                           // the leader ends the partners' game and takes their counts
+            if (pr[rank].team_broken) break;
             if (!partner) {
-                if (lane == 0) ws.pair_cmd = PAIR_GAME_END;
-                if (!pair_sync(pr, 0, &p.scratch[kStatusWord], lane)) break;
+                if (lane == 0) ws.team_cmd = TEAM_GAME_END;
+                if (!team_sync(pr, 0, &p.scratch[kStatusWord], lane)) break;
             } else {
                 uint32_t const own = __reduce_add_sync(FULL_MASK, evals);
                 if (lane == 0) pr[rank].rec[0][X_EVALS] = own;
             }
-            if (!pair_sync(pr, rank, &p.scratch[kStatusWord], lane)) break;
+            if (!team_sync(pr, rank, &p.scratch[kStatusWord], lane)) break;
             if (partner) continue;
         }
         evals = __reduce_add_sync(FULL_MASK, evals);
-        if (PAIR)
+        if (TEAMED)
 #pragma unroll 1
             for (int m = 1; m < TEAM; ++m) evals += pr[m].rec[0][X_EVALS];
         if (lane == 0) {
