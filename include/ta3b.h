@@ -204,6 +204,12 @@ int ta3b_variant_info(int variant, uint32_t* warps_per_block, uint32_t* min_bloc
  * ta3b_handoff_info reports how many games the context's last launch handed over
  * (synchronises the context's stream). */
 int ta3b_set_tail_handoff(ta3b_ctx* ctx, int on);
+/* Tests of the team kernels' bounded waits (no GPU fault involved): with flag 1
+ * the partner warps of every team leave at launch start, so each leader's first
+ * team wait runs out after 1 s; the launch ends, the call returns
+ * TA3B_ERR_DEVICE ("kernel reported status 4") and the context stays usable.
+ * 0 (the default) turns it off. Affects launches that run a team kernel. */
+int ta3b_set_test_flags(ta3b_ctx* ctx, uint32_t flags);
 int ta3b_handoff_info(ta3b_ctx* ctx, uint32_t* games_out);
 int ta3b_variant_warps_per_game(int variant);
 int ta3b_select_variant(ta3b_ctx* ctx, int variant);

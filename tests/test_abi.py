@@ -183,3 +183,9 @@ def test_noalloc_sim_bound_is_checked_before_any_device_call(lib):
 
 def test_status_query_rejects_a_null_context(lib):
     assert lib.ta3b_device_status(None, None) == -1
+
+
+def test_context_settings_reject_a_null_context(lib):
+    assert lib.ta3b_set_test_flags(None, 0) == -1
+    assert lib.ta3b_set_tail_handoff(None, 1) == -1
+    assert lib.ta3b_handoff_info(None, None) == -1

@@ -593,6 +593,8 @@ struct Params {
     uint32_t ckpt_cap;
     uint32_t handoff_at;               // hand-off flavour: hand the games over when at most this many play
     uint32_t resume;                   // paired kernel: play the checkpointed games instead of the sims
+    uint32_t test_flags;               // tests only: bit 0 = team partners leave at launch start, so
+                                       // the leaders' first team wait runs out (status bit 4)
 };
 
 // A game handed from the single-warp kernel to the paired kernel at a move boundary.
@@ -1132,6 +1134,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
     }
     if (HANDOFF && lane == 0) ws.eng.over = 0;                 // (read after the game loop)
     __syncthreads();
+    if (TEAMED && partner && (p.test_flags & 1u)) return;      // (no later block barrier)
     Luts const lut{s_lut.fast, s_lut.move};
     // the widened network's per-warp hidden-unit buffers follow the WARPS warp blocks
     float* const hb = WIDE ? reinterpret_cast<float*>(dyn_smem + WARPS * sizeof(WarpShared)) +
@@ -1440,6 +1443,7 @@ struct ta3b_ctx {
     bool auto_small = true;                      // small v11 batches run the paired kernel (until a variant is selected)
     uint32_t small_grid = 0;                     // its grid, set up on first use
     uint32_t tiny_grid = 0;                      // the teams-of-four kernel's grid (the smallest batches)
+    uint32_t test_flags = 0;                     // ta3b_set_test_flags
     bool handoff = true;                         // the default variant hands its launch's tail to the paired kernel
     uint32_t handoff_grid = 0;                   // the hand-off flavour's grid, set up on first use
     Checkpoint* d_ckpt = nullptr;                // the hand-off's checkpoints: one per paired-kernel game slot
@@ -1597,6 +1601,7 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     Params p2 = prm;
     p2.warps_active = spread ? (sims + grid - 1) / grid * (warps / games) : 0u;
     p2.budget_ns = ctx->budget_ns;
+    p2.test_flags = ctx->test_flags;
     // the default variant on a full batch: its launch's tail (at most one paired-kernel slot's worth
     // of games still playing) is checkpointed and finished by the paired kernel, two warps a game
     bool const handoff = ctx->handoff && ctx->d_ckpt && v == &kVariants[kDefaultVariant] && !spread;
@@ -1946,6 +1951,12 @@ int ta3b_core_selftest(uint32_t const* recs, uint32_t num_recs, uint32_t const* 
         g_create_error = std::string("core selftest: ") + cudaGetErrorString(e);
         return TA3B_ERR_CUDA;
     }
+    return TA3B_OK;
+}
+
+int ta3b_set_test_flags(ta3b_ctx* ctx, uint32_t flags) {
+    if (!ctx || (flags & ~1u)) return ctx ? fail(ctx, TA3B_ERR_ARG, "unknown test flag") : TA3B_ERR_ARG;
+    ctx->test_flags = flags;
     return TA3B_OK;
 }
 

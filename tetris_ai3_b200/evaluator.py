@@ -33,6 +33,7 @@ _lib = None
 EXPORTS = ["ta3b_create", "ta3b_destroy", "ta3b_last_error", "ta3b_eval", "ta3b_eval_islands", "ta3b_eval_device",
            "ta3b_eval_trace", "ta3b_eval_timed", "ta3b_simulate_seeds", "ta3b_launch_info", "ta3b_num_variants", "ta3b_variant_info",
            "ta3b_variant_warps_per_game", "ta3b_set_tail_handoff", "ta3b_handoff_info",
+           "ta3b_set_test_flags",
            "ta3b_select_variant", "ta3b_core_selftest", "ta3b_eval_device_noalloc", "ta3b_set_time_budget",
            "ta3b_device_status", "ta3b_noalloc_status"]
 
@@ -72,6 +73,7 @@ def library(path: str | None = None) -> C.CDLL:
     lib.ta3b_variant_warps_per_game.argtypes = [C.c_int]
     lib.ta3b_set_tail_handoff.argtypes = [vp, C.c_int]
     lib.ta3b_handoff_info.argtypes = [vp, vp]
+    lib.ta3b_set_test_flags.argtypes = [vp, u32]
     lib.ta3b_select_variant.argtypes = [vp, C.c_int]
     lib.ta3b_set_time_budget.argtypes = [vp, C.c_double]
     lib.ta3b_core_selftest.argtypes = [vp, u32, vp, u32, vp, vp, vp, vp, vp, vp]
@@ -267,6 +269,10 @@ class ModelEvaluator:
     def set_tail_handoff(self, on: bool):
         """Hand a full batch's tail to the paired kernel (default on); off keeps every game on one warp."""
         self._check(self._lib.ta3b_set_tail_handoff(self._ctx, int(bool(on))))
+
+    def set_test_flags(self, flags: int):
+        """Tests only: 1 = team partners leave at launch start (the leaders' waits run out)."""
+        self._check(self._lib.ta3b_set_test_flags(self._ctx, flags))
 
     def handoff_games(self) -> int:
         """How many games the last launch handed to the paired kernel."""
