@@ -111,12 +111,13 @@ def test_tail_handoff_is_bit_identical(ev):
     assert sc.tobytes() == s2.tobytes() and np.array_equal(pc, p2) and np.array_equal(lc, l2)
 
 
-def test_team_wait_runs_out_and_the_context_stays_usable(ev):
+def test_team_wait_runs_out_and_the_context_stays_usable():
     """Failure detection without a GPU fault: the test flag makes every team's partners leave at
     launch start, so each leader's first team wait gives up after its 1 s limit; the call reports
     the device status, and the same context then evaluates correctly."""
     import time
-    from tetris_ai3_b200 import EvaluatorError, workload
+    from tetris_ai3_b200 import EvaluatorError, ModelEvaluator, workload
+    ev = ModelEvaluator(device=0)           # the default launch policy: a small batch runs on a team kernel
     b = workload.generation_batch(islands=1, pop=2, games=10, max_moves=60, seed=5)
     ref = ev.eval_islands(b.weights, b.seeds, b.max_moves)
     ev.set_test_flags(1)
@@ -132,6 +133,7 @@ def test_team_wait_runs_out_and_the_context_stays_usable(ev):
     out = ev.eval_islands(b.weights, b.seeds, b.max_moves)
     assert all(x.tobytes() == y.tobytes() for x, y in zip(out, ref))
     assert ev.device_status() == 0
+    ev.close()
 
 
 def test_golden_games_single_warp_kernel(ev_solo, golden_games):
