@@ -954,7 +954,11 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
         bool const leaf = stage == DEPTH - 1;
         int const kl = stage == 0 ? K0 : (stage == 1 ? K1 : K2);
         // ---- every candidate of the stage
-        LevelAcc a = level_pass<NET, KEYS, TEAM>(ws, pr[rank], lut, fw, hb, leaf, total, kl, lane, evals,
+        // team kernels reload the fast-path weights for each pass (from L1), so that they hold no
+        // registers across the team barriers
+        FastW fwl;
+        if (TEAMED) load_fast_weights(GlobalW{ws.wglobal}, fwl);
+        LevelAcc a = level_pass<NET, KEYS, TEAM>(ws, pr[rank], lut, TEAMED ? fwl : fw, hb, leaf, total, kl, lane, evals,
                                                  uint32_t(rank * WARP));
         if (TEAMED) {
             // a partner's results go through its own record area, which it never uses otherwise
@@ -1400,6 +1404,7 @@ Variant const kKeysNet[NUM_NETS] = {{eval_kernel<4, 3, 0, false, true>, 4, 3},
                                     {eval_kernel<4, 3, 32, false, true>, 4, 3}};
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kSmallVariant = 10;  // the paired kernel: the default for batches of at most 4 games per SM
+constexpr int kResumeVariant = kSmallVariant;   // the team kernel that finishes a hand-off's games
 constexpr int kTinyVariant = 11;   // teams of four: the default for batches of at most 2 games per SM
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
@@ -1442,6 +1447,7 @@ struct ta3b_ctx {
     uint32_t keys_grid[NUM_NETS] = {0, 0, 0};    // key-tracing flavours (by NetKind), set up on first use
     bool auto_small = true;                      // small v11 batches run the paired kernel (until a variant is selected)
     uint32_t small_grid = 0;                     // its grid, set up on first use
+    uint32_t resume_grid = 0;                    // the hand-off's team kernel's grid
     uint32_t tiny_grid = 0;                      // the teams-of-four kernel's grid (the smallest batches)
     uint32_t test_flags = 0;                     // ta3b_set_test_flags
     bool handoff = true;                         // the default variant hands its launch's tail to the paired kernel
@@ -1608,17 +1614,18 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     if (handoff) {
         if (!ctx->handoff_grid)
             if (int rc = setup_kernel(ctx, kHandoffVariant, NET_V11, ctx->handoff_grid, "hand-off kernel")) return rc;
-        if (!ctx->small_grid)
-            if (int rc = setup_kernel(ctx, small, NET_V11, ctx->small_grid, "paired kernel")) return rc;
+        Variant const& resume = kVariants[kResumeVariant];
+        if (!ctx->resume_grid)
+            if (int rc = setup_kernel(ctx, resume, NET_V11, ctx->resume_grid, "hand-off's team kernel")) return rc;
         p2.ckpt = ctx->d_ckpt;
         p2.ckpt_cap = ctx->ckpt_cap;
-        p2.handoff_at = ctx->ckpt_cap < ctx->small_grid * small.games() ? ctx->ckpt_cap : ctx->small_grid * small.games();
+        p2.handoff_at = ctx->ckpt_cap < ctx->resume_grid * resume.games() ? ctx->ckpt_cap : ctx->resume_grid * resume.games();
         kHandoffVariant.fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
         TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
         Params p3 = p2;
         p3.resume = 1;
         p3.warps_active = 0;
-        small.fn<<<ctx->small_grid, small.warps * 32, small.warps * warp_bytes(NET_V11), st>>>(p3);
+        resume.fn<<<ctx->resume_grid, resume.warps * 32, resume.warps * warp_bytes(NET_V11), st>>>(p3);
     } else {
         v->fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
     }
@@ -1797,12 +1804,12 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
         cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_scratch, kScratchBytes) != cudaSuccess ||
         cudaMemset(ctx->d_scratch, 0, kScratchBytes) != cudaSuccess ||
-        cudaMalloc(&ctx->d_ckpt, size_t(ctx->sms) * kVariants[kSmallVariant].games() * sizeof(Checkpoint)) != cudaSuccess) {
+        cudaMalloc(&ctx->d_ckpt, size_t(ctx->sms) * kVariants[kResumeVariant].games() * sizeof(Checkpoint)) != cudaSuccess) {
         g_create_error = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());
         ta3b_destroy(ctx);
         return nullptr;
     }
-    ctx->ckpt_cap = ctx->sms * kVariants[kSmallVariant].games();
+    ctx->ckpt_cap = ctx->sms * kVariants[kResumeVariant].games();
     int v = kDefaultVariant;
     if (c.warps_per_block || c.blocks_per_sm) {
         v = -1;
