@@ -1089,7 +1089,7 @@ __device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, 
     return true;
 }
 
-// The paired kernel's resume: the leader warp takes the checkpointed game's state.
+// A team kernel's resume: the leader warp takes the checkpointed game's state.
 __device__ __noinline__ void load_checkpoint(WarpShared* ws, Checkpoint const* c, int lane) {
     uint32_t* const e = reinterpret_cast<uint32_t*>(&ws->eng);
     uint32_t* const t = reinterpret_cast<uint32_t*>(&ws->st);
