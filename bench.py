@@ -296,7 +296,7 @@ def run_ours(args):
             ms.append(a.elapsed_time(b))
             placements += int(evals.to(torch.int64).sum().item())
     torch.cuda.synchronize()
-    kernels_per_step = ev.launch_info()["kernels"]    # 3 with the hand-offs (rebalance, then the team kernel)
+    kernels_per_step = ev.launch_info()["kernels"]    # 2 when the tail hand-off's paired kernel ran
     clocks = clk.summary()
     t_local = sum(ms) / 1000.0
     t_max, total_pl, value = reduce_timing(t_local, float(placements), dev)
@@ -338,8 +338,8 @@ def run_ours(args):
                 "peak_source": f"{sms} SMs x 4 schedulers x 32 lanes x sm_max_mhz {sm_mhz:.0f} "
                                f"(MEASURED_PEAKS.json, {kind})",
                 "ops_per_placement": ops_per_placement,
-                "ops_basis": "placements/s of the whole evaluation (with the hand-offs, the single-warp "
-                             "kernel's two launches and the paired kernel that finishes the last games); frac (the headline) counts "
+                "ops_basis": "placements/s of the whole evaluation (with the tail hand-off, the single-warp "
+                             "kernel and the paired kernel that finishes its last games); frac (the headline) counts "
                              "the reference algorithm's operations per placement (an algorithmic count, hand count "
                              "above); frac_executed counts the lane-instructions the single-warp kernel executes per "
                              "placement at full occupancy (ncu thread_inst_executed / placements)",
@@ -367,9 +367,9 @@ def run_ours(args):
                 "clocks": clocks, "roofline": roof, "cpu_baseline": cpu,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": e2e_steps},
-                # per step: the evaluation kernels (the single-warp kernel and, with the hand-offs,
-                # its rebalanced second launch and the paired kernel that finishes the tail; the
-                # widened model adds its weight-repack kernel)
+                # per step: the evaluation kernels (the single-warp kernel and, with the tail
+                # hand-off, the paired kernel that finishes its tail; the widened model adds its
+                # weight-repack kernel)
                 "gpu_launches": args.steps * (kernels_per_step + (1 if wide else 0))}
         print(json.dumps(line), flush=True)
     if world > 1:

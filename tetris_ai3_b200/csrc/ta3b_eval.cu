@@ -40,10 +40,8 @@ constexpr uint32_t FULL_MASK = 0xFFFFFFFFu;
 constexpr int kStatusWord = 2;
 // the tail hand-off (single-warp kernel -> paired kernel): warps that found no sim, the hand-off
 // flag, games checkpointed, and the paired kernel's ticket over the checkpoints
-// hand-off level L (0: single warp -> single warp, spread evenly; 1: -> the team kernel) keeps
-// four words at kHandWords + 4 L: warps done, the flag, games checkpointed, the resume ticket
-constexpr int kHandWords = 4, kDoneWord = 0, kHandoffWord = 1, kCkptCountWord = 2, kCkptTicketWord = 3;
-constexpr size_t kScratchBytes = (kHandWords + 8) * 4;
+constexpr int kDoneWord = 3, kHandoffWord = 4, kCkptCountWord = 5, kCkptTicketWord = 6;
+constexpr size_t kScratchBytes = 32;
 constexpr uint32_t kNoSim = 0xFFFFFFFFu;                 // never a sim index: sims <= 2^32 - 1
 constexpr uint64_t kMaxSims = 0xFFFFFFFFull;
 
@@ -591,18 +589,10 @@ struct Params {
     uint32_t num_games, models_per_island, max_moves, total_sims;
     uint32_t warps_active;             // 0, or the warps of each block that play (a batch smaller than
                                        // the grid's slots is spread over every SM); the rest take no sim
-    // the hand-off (HANDOFF flavour): its level's words, where it checkpoints (out_cap slots), and
-    // the count of playing warps at which it hands its games over
-    uint32_t* hand_words;
-    struct Checkpoint* ckpt_out;
-    uint32_t out_cap;
-    uint32_t handoff_at;
-    // resume (the hand-off flavour or a team kernel): play the games the previous level checkpointed
-    // (in_words: that level's words) instead of the sims
-    uint32_t resume;
-    uint32_t* in_words;
-    struct Checkpoint const* ckpt_in;
-    uint32_t in_cap;
+    struct Checkpoint* ckpt;           // the tail hand-off's checkpoints (ckpt_cap of them)
+    uint32_t ckpt_cap;
+    uint32_t handoff_at;               // hand-off flavour: hand the games over when at most this many play
+    uint32_t resume;                   // paired kernel: play the checkpointed games instead of the sims
     uint32_t test_flags;               // tests only: bit 0 = team partners leave at launch start, so
                                        // the leaders' first team wait runs out (status bit 4)
 };
@@ -1077,10 +1067,10 @@ __device__ __forceinline__ Move search_move(WarpShared& ws, Luts lut, FastW cons
 // Checkpoint the warp's game for the paired kernel: engine and stats, the sim (parked in the warp's
 // team_sim word), its moves (= pieces placed: the game goes on, so no move failed) and evaluation
 // count (the provisional result the warp wrote). false when the array is full.
-__device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* hand, Checkpoint* ckpt, uint32_t cap,
+__device__ __noinline__ bool save_checkpoint(WarpShared* ws, uint32_t* scratch, Checkpoint* ckpt, uint32_t cap,
                                              uint32_t const* evals, int lane) {
     uint32_t idx = 0;
-    if (lane == 0) idx = atomicAdd(&hand[kCkptCountWord], 1u);
+    if (lane == 0) idx = atomicAdd(&scratch[kCkptCountWord], 1u);
     idx = __shfl_sync(FULL_MASK, idx, 0);
     if (idx >= cap) return false;
     Checkpoint* const c = ckpt + idx;
@@ -1117,11 +1107,10 @@ __device__ __noinline__ void load_checkpoint(WarpShared* ws, Checkpoint const* c
 // takes the tickets, commits the moves and writes the results, the others run their share of
 // every candidate pass (search_move's team mode); results are the single-warp kernel's, bit for
 // bit. With p.resume it plays the games a HANDOFF launch checkpointed.
-// HANDOFF: the launch hands its games on. A warp that finds no sim (or checkpoint) left counts
-// itself done; when at most p.handoff_at warps still play, it raises its level's flag, and every
-// playing warp then checkpoints its game at its next move boundary (checked every 4th move) and
-// ends. The next launch on the same stream resumes those games: the hand-off flavour again (with
-// p.resume), spread evenly over the SMs, or the team kernel for the launch's last games.
+// HANDOFF: the launch's tail goes to a team kernel. A warp that finds no sim left counts itself
+// done; when at most p.handoff_at warps still play, it raises the hand-off flag, and every playing
+// warp then checkpoints its game at its next move boundary (checked every 4th move) and ends; the
+// team kernel, launched next on the same stream, finishes those games.
 template <int WARPS, int MINB, int NET = 0, bool BUDGET = false, bool KEYS = false, int TEAM = 1,
           bool HANDOFF = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
@@ -1164,13 +1153,13 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t sim = 0, ck = 0;
         if (!partner && lane == 0) {
             sim = kNoSim;
-            if ((TEAMED || HANDOFF) && p.resume) {
+            if (TEAMED && p.resume) {
                 // the checkpointed games, spread over the blocks
-                uint32_t n = *reinterpret_cast<volatile uint32_t*>(&p.in_words[kCkptCountWord]);
-                n = n < p.in_cap ? n : p.in_cap;
+                uint32_t n = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kCkptCountWord]);
+                n = n < p.ckpt_cap ? n : p.ckpt_cap;
                 if ((threadIdx.x >> 5) / uint32_t(TEAM) < (n + gridDim.x - 1) / gridDim.x) {
-                    ck = atomicAdd(&p.in_words[kCkptTicketWord], 1u);
-                    if (ck < n) sim = p.ckpt_in[ck].sim;
+                    ck = atomicAdd(&p.scratch[kCkptTicketWord], 1u);
+                    if (ck < n) sim = p.ckpt[ck].sim;
                 }
             } else if (!p.warps_active || (threadIdx.x >> 5) < p.warps_active) {
                 // (a warp beyond the block's playing warps takes no ticket: the batch is spread over the SMs)
@@ -1179,8 +1168,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             }
             if (HANDOFF && sim == kNoSim) {
                 uint32_t const total = gridDim.x * (p.warps_active ? p.warps_active : uint32_t(WARPS));
-                uint32_t const done = atomicAdd(&p.hand_words[kDoneWord], 1u) + 1u;
-                if (total - done <= p.handoff_at) atomicExch(&p.hand_words[kHandoffWord], 1u);
+                uint32_t const done = atomicAdd(&p.scratch[kDoneWord], 1u) + 1u;
+                if (total - done <= p.handoff_at) atomicExch(&p.scratch[kHandoffWord], 1u);
             }
         }
         if (TEAMED) {                                                // the leader hands the sim to its partners
@@ -1195,7 +1184,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         uint32_t const island = mdl / p.models_per_island;
         uint64_t const seed = p.seeds[size_t(island) * p.num_games + g];
         float const* wsrc = p.weights + size_t(mdl) * (WIDE ? WideNet<HW>::STRIDE : NPARAMS);
-        bool const resumed = (TEAMED || HANDOFF) && p.resume;
+        bool const resumed = TEAMED && p.resume;
         if (p.timing && lane == 0 && !resumed) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -1212,7 +1201,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
                 if (HANDOFF) ws.team_sim = sim;                    // (read by the hand-off's checkpoint)
             }
             if (resumed) {
-                Checkpoint const* const c = p.ckpt_in + __shfl_sync(FULL_MASK, ck, 0);
+                Checkpoint const* const c = p.ckpt + __shfl_sync(FULL_MASK, ck, 0);
                 load_checkpoint(&ws, c, lane);
                 moves = c->moves;
                 if (lane == 0) evals = c->evals;
@@ -1251,7 +1240,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
             if (ws.eng.over == 2) break;
             if (HANDOFF && (moves & 3u) == 0 && moves < p.max_moves && !ws.eng.over) {
                 uint32_t f = 0;
-                if (lane == 0) f = *reinterpret_cast<volatile uint32_t*>(&p.hand_words[kHandoffWord]);
+                if (lane == 0) f = *reinterpret_cast<volatile uint32_t*>(&p.scratch[kHandoffWord]);
                 if (__shfl_sync(FULL_MASK, f, 0)) {
                     if (lane == 0) ws.eng.over = 4;                  // handed over after the game loop
                     __syncwarp();
@@ -1304,12 +1293,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB) eval_kernel(Params p) {
         __syncwarp();
         if (BUDGET && ws.eng.over == 3) break;                   // out of time: take no further sim
     }
-    // The next level finishes a handed-over game (over = 4; the game's results written above are
-    // provisional: the next level overwrites them). At most handoff_at <= out_cap games are
+    // The paired kernel finishes a handed-over game (over = 4; the game's results written above are
+    // provisional: the paired kernel overwrites them). At most handoff_at <= ckpt_cap games are
     // still playing when the flag rises, so a full array is an error.
     if (HANDOFF && ws.eng.over == 4) {
         __syncwarp();
-        if (!save_checkpoint(&ws, p.hand_words, p.ckpt_out, p.out_cap, p.evals, lane) && lane == 0)
+        if (!save_checkpoint(&ws, p.scratch, p.ckpt, p.ckpt_cap, p.evals, lane) && lane == 0)
             atomicOr(&p.scratch[kStatusWord], 8u);
     }
 }
@@ -1416,7 +1405,6 @@ Variant const kKeysNet[NUM_NETS] = {{eval_kernel<4, 3, 0, false, true>, 4, 3},
 constexpr int kNoAllocVariant = 1;   // the allocation-free entry point keeps its fixed 4 x 4 launch shape
 constexpr int kSmallVariant = 10;  // the paired kernel: the default for batches of at most 4 games per SM
 constexpr int kResumeVariant = kSmallVariant;   // the team kernel that finishes a hand-off's games
-constexpr uint32_t kRebalancePerSm = 12;          // the rebalancing hand-off: at most this many games per SM left
 constexpr int kTinyVariant = 11;   // teams of four: the default for batches of at most 2 games per SM
 constexpr int kDefaultVariant = 7;   // 16 warps, 1 block/SM: the autotuner's pick on the full generation and the stress batch
 
@@ -1464,10 +1452,8 @@ struct ta3b_ctx {
     uint32_t test_flags = 0;                     // ta3b_set_test_flags
     bool handoff = true;                         // the default variant hands its launch's tail to the paired kernel
     uint32_t handoff_grid = 0;                   // the hand-off flavour's grid, set up on first use
-    Checkpoint* d_ckpt = nullptr;                // level 1's checkpoints: one per team-kernel game slot
+    Checkpoint* d_ckpt = nullptr;                // the hand-off's checkpoints: one per paired-kernel game slot
     uint32_t ckpt_cap = 0;
-    Checkpoint* d_ckpt0 = nullptr;               // level 0's (the rebalancing hand-off): one per warp slot
-    uint32_t ckpt0_cap = 0;
     uint64_t* d_keys = nullptr;                  // per move the two largest final keys (tracing)
     size_t cap_keys = 0;
     uint32_t last_grid = 0, last_warps = 0;   // the most recent launch's shape (0: none yet)
@@ -1624,54 +1610,29 @@ int launch(ta3b_ctx* ctx, Params const& prm, cudaStream_t st, int ni = NET_V11) 
     p2.test_flags = ctx->test_flags;
     // the default variant on a full batch: its launch's tail (at most one paired-kernel slot's worth
     // of games still playing) is checkpointed and finished by the paired kernel, two warps a game
-    bool const handoff = ctx->handoff && ctx->d_ckpt && ctx->d_ckpt0 && v == &kVariants[kDefaultVariant] && !spread;
+    bool const handoff = ctx->handoff && ctx->d_ckpt && v == &kVariants[kDefaultVariant] && !spread;
     if (handoff) {
         if (!ctx->handoff_grid)
             if (int rc = setup_kernel(ctx, kHandoffVariant, NET_V11, ctx->handoff_grid, "hand-off kernel")) return rc;
         Variant const& resume = kVariants[kResumeVariant];
         if (!ctx->resume_grid)
             if (int rc = setup_kernel(ctx, resume, NET_V11, ctx->resume_grid, "hand-off's team kernel")) return rc;
-        uint32_t* const w0 = prm.scratch + kHandWords;             // level 0's words
-        uint32_t* const w1 = w0 + 4;                              // level 1's
-        uint32_t const team_slots = ctx->resume_grid * resume.games();
-        // level 0: when at most kRebalancePerSm games per SM are left, checkpoint them all and
-        // resume them spread evenly over the SMs (the SMs' remaining work differs by +-25 % when
-        // the queue drains); level 1: at most one team-kernel slot's worth left -> the team kernel
-        uint32_t const rebalance_at = ctx->sms * kRebalancePerSm;
-        p2.hand_words = w0;
-        p2.ckpt_out = ctx->d_ckpt0;
-        p2.out_cap = ctx->ckpt0_cap;
-        p2.handoff_at = rebalance_at < ctx->ckpt0_cap ? rebalance_at : ctx->ckpt0_cap;
+        p2.ckpt = ctx->d_ckpt;
+        p2.ckpt_cap = ctx->ckpt_cap;
+        p2.handoff_at = ctx->ckpt_cap < ctx->resume_grid * resume.games() ? ctx->ckpt_cap : ctx->resume_grid * resume.games();
         kHandoffVariant.fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
         TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
         Params p3 = p2;
-        p3.warps_active = 0;
         p3.resume = 1;
-        p3.in_words = w0;
-        p3.ckpt_in = ctx->d_ckpt0;
-        p3.in_cap = ctx->ckpt0_cap;
-        p3.hand_words = w1;
-        p3.ckpt_out = ctx->d_ckpt;
-        p3.out_cap = ctx->ckpt_cap;
-        p3.handoff_at = ctx->ckpt_cap < team_slots ? ctx->ckpt_cap : team_slots;
-        kHandoffVariant.fn<<<ctx->handoff_grid, warps * 32, warps * warp_bytes(ni), st>>>(p3);
-        TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
-        Params p4 = p3;
-        p4.in_words = w1;
-        p4.ckpt_in = ctx->d_ckpt;
-        p4.in_cap = ctx->ckpt_cap;
-        p4.hand_words = nullptr;
-        p4.ckpt_out = nullptr;
-        p4.out_cap = 0;
-        p4.handoff_at = 0;
-        resume.fn<<<ctx->resume_grid, resume.warps * 32, resume.warps * warp_bytes(NET_V11), st>>>(p4);
+        p3.warps_active = 0;
+        resume.fn<<<ctx->resume_grid, resume.warps * 32, resume.warps * warp_bytes(NET_V11), st>>>(p3);
     } else {
         v->fn<<<grid, warps * 32, warps * warp_bytes(ni), st>>>(p2);
     }
     TA3B_CUDA(ctx, cudaGetLastError(), "kernel launch");
     ctx->last_grid = grid;
     ctx->last_warps = warps;
-    ctx->last_kernels = handoff ? 3u : 1u;
+    ctx->last_kernels = handoff ? 2u : 1u;
     return TA3B_OK;
 }
 
@@ -1843,14 +1804,12 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
         cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_scratch, kScratchBytes) != cudaSuccess ||
         cudaMemset(ctx->d_scratch, 0, kScratchBytes) != cudaSuccess ||
-        cudaMalloc(&ctx->d_ckpt, size_t(ctx->sms) * kVariants[kResumeVariant].games() * sizeof(Checkpoint)) != cudaSuccess ||
-        cudaMalloc(&ctx->d_ckpt0, size_t(ctx->sms) * kHandoffVariant.warps * sizeof(Checkpoint)) != cudaSuccess) {
+        cudaMalloc(&ctx->d_ckpt, size_t(ctx->sms) * kVariants[kResumeVariant].games() * sizeof(Checkpoint)) != cudaSuccess) {
         g_create_error = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());
         ta3b_destroy(ctx);
         return nullptr;
     }
     ctx->ckpt_cap = ctx->sms * kVariants[kResumeVariant].games();
-    ctx->ckpt0_cap = ctx->sms * kHandoffVariant.warps;
     int v = kDefaultVariant;
     if (c.warps_per_block || c.blocks_per_sm) {
         v = -1;
@@ -1880,7 +1839,7 @@ void ta3b_destroy(ta3b_ctx* ctx) {
     cudaSetDevice(ctx->device);
     void* bufs[] = {ctx->d_w, ctx->d_seeds, ctx->d_score, ctx->d_pieces, ctx->d_lines, ctx->d_evals,
                     ctx->d_trace, ctx->d_nmoves, ctx->d_board, ctx->d_scratch, ctx->d_timing, ctx->d_wpad,
-                    ctx->d_keys, ctx->d_ckpt, ctx->d_ckpt0};
+                    ctx->d_keys, ctx->d_ckpt};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -2017,8 +1976,7 @@ int ta3b_set_tail_handoff(ta3b_ctx* ctx, int on) {
 int ta3b_handoff_info(ta3b_ctx* ctx, uint32_t* games_out) {
     if (!ctx || !games_out) return TA3B_ERR_ARG;
     uint32_t n = 0;
-    TA3B_CUDA(ctx, cudaMemcpyAsync(&n, ctx->d_scratch + kHandWords + 4 + kCkptCountWord, sizeof n,
-                                   cudaMemcpyDeviceToHost, ctx->stream),
+    TA3B_CUDA(ctx, cudaMemcpyAsync(&n, ctx->d_scratch + kCkptCountWord, sizeof n, cudaMemcpyDeviceToHost, ctx->stream),
               "read hand-off count");
     TA3B_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "read hand-off count");
     *games_out = n < ctx->ckpt_cap ? n : ctx->ckpt_cap;
