@@ -354,6 +354,22 @@ def test_generation_graph_with_tail_handoff(ev):
         assert sc.tobytes() == s2.tobytes() and np.array_equal(pc, p2) and np.array_equal(lc, l2)
 
 
+def test_device_entry_point_with_the_hand_off_and_no_optional_outputs(ev):
+    """ta3b_eval_device on a full batch (tail hand-off) with only the score buffer: the handed-over
+    games carry no evaluation count, and the scores equal the host entry point's."""
+    import torch
+    from tetris_ai3_b200 import workload
+    b = workload.generation_batch(islands=4, pop=50, games=50, max_moves=120, seed=44)
+    w = torch.from_numpy(b.weights).cuda()
+    s = torch.from_numpy(b.seeds.view(np.int64)).cuda()
+    score = torch.empty(w.shape[0] * b.seeds.shape[1], dtype=torch.float32, device="cuda")
+    ev.eval_device(w, s, b.max_moves, score, num_islands=4)
+    torch.cuda.synchronize()
+    assert ev.device_status() == 0 and ev.launch_info()["kernels"] == 2 and ev.handoff_games() > 0
+    sc, _, _ = ev.eval_islands(b.weights, b.seeds, b.max_moves)
+    assert score.cpu().numpy().tobytes() == sc.tobytes()
+
+
 def test_time_budget_stops_the_launch_and_keeps_the_context(ev):
     """A budget far below the batch's run time ends the launch early with
     TA3B_ERR_TIMEOUT (no fault); without a budget the same context then scores
