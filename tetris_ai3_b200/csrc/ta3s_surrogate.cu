@@ -668,8 +668,16 @@ ta3s_model* ta3s_create(int device, uint32_t seed) {
     for (int c = 0; c < 128; ++c) stats[128 + c] = 1.f;
     m->x_mean.assign(IN, 0.f);
     m->x_inv_std.assign(IN, 1.f);
-    cudaMemcpy(m->d_stats, stats.data(), 256 * 4, cudaMemcpyHostToDevice);
-    cudaMemset(m->d_status, 0, 4);
+    // every copy and fill goes on the model's stream: its kernels run on a non-blocking stream, which
+    // does not wait for work on the legacy default stream (a pageable cudaMemcpy can even return
+    // before its DMA has landed)
+    if (cudaMemcpyAsync(m->d_stats, stats.data(), 256 * 4, cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+        cudaMemsetAsync(m->d_status, 0, 4, m->stream) != cudaSuccess ||
+        cudaStreamSynchronize(m->stream) != cudaSuccess) {
+        g_err = "ta3s_create: initial copies failed";
+        ta3s_destroy(m);
+        return nullptr;
+    }
     return m;
 }
 
@@ -689,9 +697,10 @@ const char* ta3s_last_error(const ta3s_model* m) { return m ? m->err.c_str() : g
 int ta3s_set_params(ta3s_model* m, const float* params) {
     if (!m || !params) return fail(m, "ta3s_set_params: null argument");
     TA3S_CUDA(m, cudaSetDevice(m->device), "set device");
-    TA3S_CUDA(m, cudaMemcpy(m->d_param, params, NPARAM * 4, cudaMemcpyHostToDevice), "params");
-    TA3S_CUDA(m, cudaMemset(m->d_m, 0, NPARAM * 4), "adam m");
-    TA3S_CUDA(m, cudaMemset(m->d_v, 0, NPARAM * 4), "adam v");
+    // on the model's (non-blocking) stream, ahead of the refresh kernel that reads them
+    TA3S_CUDA(m, cudaMemcpyAsync(m->d_param, params, NPARAM * 4, cudaMemcpyHostToDevice, m->stream), "params");
+    TA3S_CUDA(m, cudaMemsetAsync(m->d_m, 0, NPARAM * 4, m->stream), "adam m");
+    TA3S_CUDA(m, cudaMemsetAsync(m->d_v, 0, NPARAM * 4, m->stream), "adam v");
     m->adam_t = 0;
     refresh_kernel<<<(128 * 128 + 255) / 256, 256, 0, m->stream>>>(m->d_param, m->d_w1b, m->d_w2b);
     TA3S_CUDA(m, cudaGetLastError(), "refresh");

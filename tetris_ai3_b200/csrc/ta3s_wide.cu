@@ -641,8 +641,11 @@ ta3w_model* ta3w_create(int device, uint32_t in_dim, uint32_t hidden, uint32_t s
     std::fill(stats.begin() + d.inp, stats.end(), 1.f);
     m->x_mean.assign(size_t(d.in), 0.f);
     m->x_inv_std.assign(size_t(d.in), 1.f);
-    if (cudaMemcpy(m->d_stats, stats.data(), stats.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemset(m->d_status, 0, 4) != cudaSuccess)
+    // on the model's stream: its kernels run on a non-blocking stream, which does not wait for the
+    // legacy default stream (a pageable cudaMemcpy can even return before its DMA has landed)
+    if (cudaMemcpyAsync(m->d_stats, stats.data(), stats.size() * 4, cudaMemcpyHostToDevice, m->stream) != cudaSuccess ||
+        cudaMemsetAsync(m->d_status, 0, 4, m->stream) != cudaSuccess ||
+        cudaStreamSynchronize(m->stream) != cudaSuccess)
         return bad("init copies");
     return m;
 }
@@ -671,9 +674,10 @@ int ta3w_set_params(ta3w_model* m, const float* params) {
     std::vector<float> p(params, params + d.n);
     for (int o = 0; o < d.h; ++o)       // padding columns of W1 stay zero
         for (int i = d.in; i < d.inp; ++i) p[size_t(d.w1) + size_t(o) * d.inp + i] = 0.f;
-    TA3W_CUDA(m, cudaMemcpy(m->d_param, p.data(), size_t(d.n) * 4, cudaMemcpyHostToDevice), "params");
-    TA3W_CUDA(m, cudaMemset(m->d_m, 0, size_t(d.n) * 4), "adam m");
-    TA3W_CUDA(m, cudaMemset(m->d_v, 0, size_t(d.n) * 4), "adam v");
+    // on the model's (non-blocking) stream, ahead of the refresh kernel that reads them
+    TA3W_CUDA(m, cudaMemcpyAsync(m->d_param, p.data(), size_t(d.n) * 4, cudaMemcpyHostToDevice, m->stream), "params");
+    TA3W_CUDA(m, cudaMemsetAsync(m->d_m, 0, size_t(d.n) * 4, m->stream), "adam m");
+    TA3W_CUDA(m, cudaMemsetAsync(m->d_v, 0, size_t(d.n) * 4, m->stream), "adam v");
     m->adam_t = 0;
     refresh_kernel<<<unsigned((d.w3 + 255) / 256), 256, 0, m->stream>>>(m->d_param, d.w2, d.w3, m->d_w1b, m->d_w2b);
     TA3W_CUDA(m, cudaGetLastError(), "refresh");
