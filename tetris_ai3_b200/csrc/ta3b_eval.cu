@@ -1803,7 +1803,8 @@ ta3b_ctx* ta3b_create(ta3b_config const* cfg) {
     if (cudaSetDevice(c.device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&ctx->d_scratch, kScratchBytes) != cudaSuccess ||
-        cudaMemset(ctx->d_scratch, 0, kScratchBytes) != cudaSuccess ||
+        cudaMemsetAsync(ctx->d_scratch, 0, kScratchBytes, ctx->stream) != cudaSuccess ||   // (the context's stream
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess ||                              // orders every later use)
         cudaMalloc(&ctx->d_ckpt, size_t(ctx->sms) * kVariants[kResumeVariant].games() * sizeof(Checkpoint)) != cudaSuccess) {
         g_create_error = std::string("context setup: ") + cudaGetErrorString(cudaGetLastError());
         ta3b_destroy(ctx);
