@@ -97,8 +97,9 @@ int ta3b_eval_islands(ta3b_ctx* ctx, const float* weights, uint32_t num_islands,
                       float* score_out, uint32_t* pieces_out, uint32_t* lines_out);
 
 /* Device-resident variant of ta3b_eval_islands: every pointer is device memory;
- * enqueued on `stream` (a cudaStream_t, NULL = the context's stream) and NOT
- * synchronised. evals_out (may be NULL) receives per-sim counts of evaluated
+ * enqueued on `stream` (a cudaStream_t, NULL = the context's stream, a
+ * non-blocking stream that does not wait for the legacy default stream: inputs
+ * written elsewhere must be complete first) and NOT synchronised. evals_out (may be NULL) receives per-sim counts of evaluated
  * beam placements (value-model calls). Used for HBM-resident batches and CUDA
  * graph capture. With the widened network (num_params = TA3B_NUM_PARAMS_WIDE)
  * the call first repacks the weights into the kernel's layout (16-byte aligned,
