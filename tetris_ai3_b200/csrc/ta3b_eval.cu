@@ -1445,7 +1445,7 @@ struct ta3b_ctx {
     uint32_t net_grid[NUM_NETS] = {0, 0, 0};     // widened-network kernels (by NetKind), set up on first use
     uint32_t budget_grid[NUM_NETS] = {0, 0, 0};  // budget flavours (by NetKind), set up on first use
     uint32_t keys_grid[NUM_NETS] = {0, 0, 0};    // key-tracing flavours (by NetKind), set up on first use
-    bool auto_small = true;                      // small v11 batches run the paired kernel (until a variant is selected)
+    bool auto_small = true;                      // small v11 batches run a team kernel (until a variant is selected)
     uint32_t small_grid = 0;                     // its grid, set up on first use
     uint32_t resume_grid = 0;                    // the hand-off's team kernel's grid
     uint32_t tiny_grid = 0;                      // the teams-of-four kernel's grid (the smallest batches)
