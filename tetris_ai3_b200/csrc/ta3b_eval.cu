@@ -2054,7 +2054,7 @@ static_assert(kScratchBytes <= sizeof(g_noalloc_scratch), "the work-queue words 
 constexpr int kNoAllocMaxDevices = 64;
 struct NoAllocDevice {
     uint32_t* scratch;   // device address of g_noalloc_scratch on this device
-    uint32_t grid;
+    uint32_t grid, sms;
     bool ready;
 };
 NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
@@ -2101,6 +2101,7 @@ extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_isl
                 return fail_static(TA3B_ERR_CUDA, "occupancy query failed");
             d.scratch = static_cast<uint32_t*>(ptr);
             d.grid = uint32_t(sms) * uint32_t(per_sm);
+            d.sms = uint32_t(sms);
             d.ready = true;
         }
     }
@@ -2121,8 +2122,12 @@ extern "C" int ta3b_eval_device_noalloc(float const* d_weights, uint32_t num_isl
     prm.models_per_island = models_per_island;
     prm.max_moves = max_moves;
     prm.total_sims = uint32_t(sims);
+    // a batch that one block per SM can hold is spread over every SM (as on the context path)
     uint32_t const need = uint32_t((sims + var.warps - 1) / var.warps);
-    var.fn<<<need < d.grid ? need : d.grid, var.warps * 32, dyn, st>>>(prm);
+    bool const spread = sims < uint64_t(d.sms) * var.warps;
+    uint32_t const grid = spread ? uint32_t(sims < d.sms ? sims : d.sms) : (need < d.grid ? need : d.grid);
+    if (spread) prm.warps_active = uint32_t((sims + grid - 1) / grid);
+    var.fn<<<grid, var.warps * 32, dyn, st>>>(prm);
     if (cudaGetLastError() != cudaSuccess) return fail_static(TA3B_ERR_CUDA, "kernel launch failed");
     return TA3B_OK;
 }
